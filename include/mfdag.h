@@ -1,0 +1,220 @@
+/*
+ * mfdag.h -- C ABI of the B200 (sm_100a) numeric phase for the supernodal
+ * multifrontal Cholesky solver to-mo-ki/multifrontal-DAG.
+ *
+ * Two layers:
+ *
+ *  1. Handle API (mfd_*): the drop-in boundary.  A handle owns all device
+ *     memory of one analysed system (or of a batch of independent systems):
+ *     factor panels and update matrices resident in HBM, the device-built index
+ *     maps, and the launch plan.  Plain pointers and sizes only; integer arrays
+ *     are int32 with the reference's 1-based values; dense values are FP64,
+ *     column-major.
+ *
+ *  2. Reference-named entry points (hppllt_*): the same calls as the
+ *     reference's public Fortran API (src/main/hppllt.f90:8-9), with the same
+ *     argument meaning and module-global single-instance state, for a C or
+ *     ISO_C_BINDING caller.  They run the host symbolic analysis in C++ and the
+ *     numeric phase on the GPU.
+ *
+ * Status codes: 0 ok; >0 = 1-based (permuted) column of the first
+ * non-positive pivot (LAPACK convention); negative = MFD_E_*.
+ */
+#ifndef MFDAG_H
+#define MFDAG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MFD_OK 0
+#define MFD_E_ARG (-1)        /* bad argument or malformed symbolic input            */
+#define MFD_E_CUDA (-2)       /* a CUDA call failed                                  */
+#define MFD_E_NOMEM (-3)      /* device or host allocation failed                    */
+#define MFD_E_TIMEOUT (-4)    /* a bounded device-side wait expired                  */
+#define MFD_E_NOCONV (-5)     /* iterative refinement did not reach the tolerance     */
+#define MFD_E_STATE (-6)      /* call out of order (e.g. solve before factorize)     */
+
+#define MFD_PREC_FP64 0       /* FP64 factor and solve                               */
+#define MFD_PREC_FP32_IR 1    /* FP32 factor + FP64 iterative refinement             */
+
+typedef struct mfd_handle mfd_handle;
+
+typedef struct {
+  int32_t nb;              /* reference option OPTION_NB (options_m.f90:4): tile size of the
+                              reference layout; used for the block-local index export        */
+  int32_t max_zero;        /* reference option OPTION_MAX_ZERO (options_m.f90:5)             */
+  int32_t precision;       /* MFD_PREC_*                                                      */
+  int32_t ir_max_iter;     /* refinement iterations (precision FP32_IR), default 20           */
+  double ir_tol;           /* target normwise backward error, default 1e-12                   */
+  int32_t use_graph;       /* 1: replay factor/solve as CUDA graphs (default 1)               */
+  int32_t device;          /* CUDA device ordinal (default 0)                                 */
+  int32_t small_front_max; /* fronts up to this order run in the fused one-CTA kernel (0=auto)*/
+  int32_t panel_width;     /* column panel of the blocked large-front factorization (0=auto) */
+  int32_t reserved[7];
+} mfd_options;
+
+/* Symbolic data exactly as the reference holds it after hppllt_analyze
+ * (hppllt_data_m.f90:14-29, hppllt.f90:56-73); all arrays 1-based int32. */
+typedef struct {
+  int32_t n, nnz, num_node;
+  const int32_t *node_ptr;  /* num_node+1 : node_sets%ptr                              */
+  const int32_t *parent;    /* num_node   : supernodal parent, 0 for the root          */
+  const int32_t *lrow_ptr;  /* num_node+1 : l_structure set                            */
+  const int32_t *lrow;      /* sum nr     : L row lists, ascending, permuted numbering */
+  const int32_t *acol_ptr;  /* n+1        : a_structure (permuted lower CCS)           */
+  const int32_t *arow;      /* nnz        : a_structure rows (any order in a column)   */
+  const int32_t *ccs_perm;  /* nnz        : entry k of a_structure takes a(ccs_perm(k)) */
+  const int32_t *perm;      /* n          : permuted position i holds original perm(i) */
+} mfd_symbolic;
+
+typedef struct {
+  int32_t iterations;       /* refinement steps taken (0 for FP64)                     */
+  int32_t converged;        /* 1 if backward_error <= ir_tol                           */
+  double backward_error;    /* ||b-Ax||_inf / (||A||_inf ||x||_inf + ||b||_inf), FP64  */
+  double residual_ref;      /* the reference driver's metric ||b-Ax||_2 / ||x||_2      */
+  double time_ms;           /* device time of the whole solve (events)                 */
+} mfd_report;
+
+typedef struct {
+  int64_t n, nnz_a, num_front, num_level;
+  int64_t cost;             /* calculate_cost (cost_calculator_m.f90:9-20): sum_f sum_{k=nr+1}^{nr+nc} k^2 */
+  int64_t nonzero;          /* count_nonzero (cost_calculator_m.f90:22-33), int64 here          */
+  int64_t panel_bytes;      /* resident factor panels                                          */
+  int64_t update_pool_bytes;/* statically planned update-matrix pool (peak of live updates)    */
+  int64_t launches_factor;  /* kernels launched by one factorize                               */
+  int64_t launches_solve;   /* kernels launched by one forward+backward solve                  */
+  int64_t max_front;        /* largest front order                                             */
+  double factor_ms;         /* device time of the last factorize (events)                      */
+  double solve_ms;          /* device time of the last solve                                   */
+  double time_info[7];      /* the reference's 7 phase timers (time_list_m.f90:3-10), seconds:
+                               ordering, analyze, factorize, solve, forward, backward,
+                               real_factorize                                                  */
+} mfd_stats;
+
+/* ---- handle API ------------------------------------------------------------ */
+
+/* Default options (FP64, graphs on, device 0). */
+void mfd_default_options(mfd_options *opt);
+
+/* Replaces the device-side half of create_data_structure (hppllt.f90:83-106):
+ * copies the symbolic arrays to the device, builds local_index, supernodal_index
+ * and block_local_index on the GPU, and plans the level schedule and memory. */
+int mfd_create(mfd_handle **h, const mfd_symbolic *sym, const mfd_options *opt);
+
+/* Batch of independent systems analysed separately (one symbolic per system):
+ * all systems share one handle, one level schedule and one launch per level. */
+int mfd_create_batch(mfd_handle **h, int32_t num_systems, const mfd_symbolic *syms, const mfd_options *opt);
+
+/* Host symbolic analysis (hppllt_analyze, hppllt.f90:24-81) + mfd_create.
+ * order_perm (new->old, 1-based) stands in for METIS_NodeND's output
+ * (hppllt.f90:47-51); NULL is the use_metis = 0 branch. */
+int mfd_analyze(mfd_handle **h, int32_t n, const int32_t *ccs_col, const int32_t *ccs_row,
+                const int32_t *order_perm, const mfd_options *opt);
+
+/* Host-only symbolic analysis (hppllt_analyze's symbolic half, no device work):
+ * the result object owns the arrays; mfd_symbolic_view fills an mfd_symbolic
+ * whose pointers stay valid until mfd_symbolic_free. */
+typedef struct mfd_analysis mfd_analysis;
+int mfd_symbolic_analyze(mfd_analysis **out, int32_t n, const int32_t *ccs_col, const int32_t *ccs_row,
+                         const int32_t *order_perm, int32_t max_zero);
+int mfd_symbolic_view(const mfd_analysis *a, mfd_symbolic *view);
+int mfd_symbolic_free(mfd_analysis *a);
+
+/* Batch analysis: system s is (n[s], ccs_col[s], ccs_row[s], order_perm[s]). */
+int mfd_analyze_batch(mfd_handle **h, int32_t num_systems, const int32_t *n, const int32_t *const *ccs_col,
+                      const int32_t *const *ccs_row, const int32_t *const *order_perm, const mfd_options *opt);
+
+/* Replaces the body of hppllt_factorize (hppllt.f90:134-149): permutate,
+ * set_zero, set_coefficient, seq/StarPU factorize.  a: original-order lower-CCS
+ * values (for a batch, systems concatenated), host or device pointer. */
+int mfd_factorize(mfd_handle *h, const double *a);
+
+/* Replaces the body of hppllt_solve (hppllt.f90:160-172): b (n x nrhs,
+ * column-major, leading dimension ldb; for a batch, systems concatenated) is
+ * overwritten with x.  Host or device pointer.  rep may be NULL. */
+int mfd_solve(mfd_handle *h, double *b, int32_t nrhs, int64_t ldb, mfd_report *rep);
+
+/* Factorize + solve in one call (the batched configuration's single launch
+ * sequence). */
+int mfd_factorize_solve(mfd_handle *h, const double *a, double *b, int32_t nrhs, int64_t ldb, mfd_report *rep);
+
+int mfd_get_stats(mfd_handle *h, mfd_stats *st);
+
+/* Export of the device-built index maps for parity checks.
+ * which: 1 local_index (sum nr), 2 supernodal_index (nnz), 3 block-local node
+ * pointer (num_node+1), 4 block pointer (groups+1), 5 parent tile numbers,
+ * 6 child tile numbers, 7 rebuilt (mod nb) local values (sum nr), 8 block
+ * offsets (get_block_offset, per group).  Returns the element count; out may
+ * be NULL to query the size.  system selects one system of a batch. */
+int64_t mfd_get_index(mfd_handle *h, int32_t system, int32_t which, int32_t *out);
+
+/* Export of the symbolic arrays held by the handle (same ids as mfd_symbolic
+ * fields: 1 node_ptr, 2 parent, 3 lrow_ptr, 4 lrow, 5 acol_ptr, 6 arow,
+ * 7 ccs_perm, 8 perm).  Returns the element count; out may be NULL. */
+int64_t mfd_get_symbolic(mfd_handle *h, int32_t system, int32_t which, int32_t *out);
+
+/* Copy the FP64 factor column block of one front to the host: rows 0..nf-1,
+ * columns 0..nc-1 of the front (row = front position, column-major, ld = nf).
+ * node is 1-based within the system.  Returns nf*nc or a negative status. */
+int64_t mfd_get_front_panel(mfd_handle *h, int32_t system, int32_t node, double *out);
+
+/* Per-kernel-class timing.  While enabled, factorize and solve run without
+ * graphs and record CUDA events around every launch on the handle's stream;
+ * each class accumulates its launches, device time and algorithmic work
+ * (flops and bytes of the algorithm, not hardware counters). */
+#define MFD_K_SMALL_FRONT 0   /* fused one-CTA fronts                         */
+#define MFD_K_ZERO 1          /* large-front zero fill                         */
+#define MFD_K_ASSEMBLE 2      /* large-front assembly of A                     */
+#define MFD_K_EXTEND_ADD 3    /* large-front extend-add                        */
+#define MFD_K_PANEL 4         /* panel POTRF + TRSM                            */
+#define MFD_K_UPDATE 5        /* trailing SYRK/GEMM update                     */
+#define MFD_K_SOLVE_SMALL 6   /* one-CTA forward/backward solves               */
+#define MFD_K_SOLVE_LARGE 7   /* blocked forward/backward solves               */
+#define MFD_K_OTHER 8         /* permutations, residuals, norms                */
+#define MFD_K_COUNT 9
+typedef struct {
+  int64_t launches;
+  double ms;
+  double flops;
+  double bytes;
+} mfd_kernel_profile;
+int mfd_set_profiling(mfd_handle *h, int32_t enable);
+int mfd_get_profile(mfd_handle *h, int32_t kind, mfd_kernel_profile *out);
+
+int mfd_destroy(mfd_handle *h);
+
+/* Last error text of this thread. */
+const char *mfd_last_error(void);
+
+/* ---- reference-named entry points (module-global state, hppllt.f90) ------- */
+
+/* hppllt_init(options(4)) (hppllt.f90:13-22): [nb, max_zero, use_starpu, use_metis].
+ * Returns 0, or -1 if noptions != 4 (the reference prints and returns). */
+int hppllt_init(const int32_t *options, int32_t noptions);
+/* Selects the arithmetic (MFD_PREC_*) of the next factorize; not in the reference. */
+int hppllt_set_precision(int32_t precision);
+/* hppllt_analyze(ccs_col, ccs_row, n) (hppllt.f90:24-81); with use_metis = 1 the
+ * ordering must be supplied first through hppllt_set_ordering. */
+int hppllt_analyze(const int32_t *ccs_col, const int32_t *ccs_row, int32_t n);
+/* Supplies the fill-reducing ordering used when use_metis = 1 (new->old, 1-based). */
+int hppllt_set_ordering(const int32_t *order_perm, int32_t n);
+/* hppllt_factorize(a) (hppllt.f90:123-150) */
+int hppllt_factorize(const double *a);
+/* hppllt_solve(b) (hppllt.f90:152-173), b in/out, length n */
+int hppllt_solve(double *b);
+/* hppllt_finalize (hppllt.f90:175-184) */
+int hppllt_finalize(void);
+double hppllt_get_time_info(int32_t num);   /* hppllt.f90:186-189 */
+int64_t hppllt_get_cost(void);              /* hppllt.f90:191-194 */
+int64_t hppllt_get_nonzero(void);           /* hppllt.f90:196-199 (int64 here) */
+int64_t hppllt_get_array_size(int32_t num); /* hppllt.f90:201-211: 1 supernode, 2 work, 3 border
+                                               (sizes of the reference's three FP64 buffers) */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MFDAG_H */

@@ -1,0 +1,1355 @@
+// Host side of the C ABI (include/mfdag.h): handle, static plan, graph-captured
+// launch sequences, iterative refinement, exports, and the reference-named
+// hppllt_* entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/mfdag.h"
+#include "analysis.hpp"
+#include "kernels.cuh"
+#include "plan.hpp"
+
+namespace mfd {
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                             \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(e_ == cudaErrorMemoryAllocation ? MFD_E_NOMEM : MFD_E_CUDA,                \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+  } while (0)
+
+constexpr int64_t kAlign = 32;  // elements; keeps every front 256-byte aligned in FP64
+int64_t align_up(int64_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    release();
+    n = count;
+    return cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+  }
+  cudaError_t upload(const std::vector<T>& v, cudaStream_t st) {
+    cudaError_t e = alloc(v.size());
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+  }
+};
+
+// first-fit allocator over a simulated address space (static memory plan)
+struct FirstFit {
+  std::map<int64_t, int64_t> free_;  // offset -> size
+  int64_t top = 0;
+  int64_t alloc(int64_t size) {
+    size = align_up(std::max<int64_t>(size, 1));
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= size) {
+        int64_t off = it->first, rest = it->second - size;
+        free_.erase(it);
+        if (rest > 0) free_[off + size] = rest;
+        return off;
+      }
+    }
+    int64_t off = top;
+    top += size;
+    return off;
+  }
+  void release(int64_t off, int64_t size) {
+    size = align_up(std::max<int64_t>(size, 1));
+    auto it = free_.emplace(off, size).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+};
+
+struct SmallBin {
+  int nf_max;
+};
+
+}  // namespace
+}  // namespace mfd
+
+using namespace mfd;
+
+struct mfd_handle {
+  int device = 0;
+  mfd_options opt{};
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // systems
+  std::vector<Symbolic> sys;
+  std::vector<int64_t> col_base, a_base;
+  std::vector<int32_t> front_base;
+  int64_t n_total = 0, nnz_total = 0;
+  int32_t num_front = 0;
+
+  // host tables
+  std::vector<HostFront> fronts;
+  std::vector<int32_t> h_child_ptr, h_child, h_lrow_off, h_a_beg;
+  std::vector<LevelPlan> levels;
+  std::vector<int32_t> h_lists;
+  std::vector<int> small_bins;
+  int64_t panel_elems = 0, upool_elems = 0, v_elems = 0, s_elems = 0;
+  int32_t max_large_count = 0, max_nf = 0;
+  int64_t cost = 0, nonzero = 0;
+
+  // device tables
+  DBuf<int32_t> d_nc, d_nr, d_first, d_parent, d_child_ptr, d_child, d_lrow_off, d_lrow, d_local, d_a_beg, d_a_src,
+      d_a_pos, d_sidx, d_lists, d_perm, d_info;
+  DBuf<int64_t> d_panel_off, d_u_off, d_v_off, d_s_off;
+  DevFronts F{};
+
+  // CSR of the permuted full matrix (residuals)
+  DBuf<int64_t> d_csr_ptr;
+  DBuf<int32_t> d_csr_col, d_csr_src;
+  DBuf<double> d_csr_val;
+
+  // numeric storage
+  bool fp32 = false;
+  void* d_panel = nullptr;
+  void* d_upool = nullptr;
+  void* d_diag = nullptr;
+  DBuf<double> d_a, d_b, d_xp, d_bp, d_r, d_norms;
+  void* d_X = nullptr;   // T, n_total x nrhs
+  void* d_V = nullptr;   // T
+  void* d_S = nullptr;   // T
+  int nrhs_cap = 0;
+
+  // block-local index export (per system)
+  std::vector<std::vector<int32_t>> bli_node_ptr, bli_block_ptr, bli_pnum, bli_cnum, bli_off, bli_val, local_sys,
+      sidx_sys;
+
+  bool factored = false;
+  int64_t launches_factor = 0, launches_solve = 0;
+  double factor_ms = 0, solve_ms = 0, anorm = 0;
+  double time_info[7] = {0, 0, 0, 0, 0, 0, 0};
+  cudaGraphExec_t g_factor = nullptr;
+  std::map<int, cudaGraphExec_t> g_solve;
+
+  // per-kernel-class profiling (graphs off while enabled)
+  bool profiling = false;
+  mfd_kernel_profile prof[MFD_K_COUNT]{};
+  struct PendingLaunch { int kind; double flops, bytes; cudaEvent_t a, b; };
+  std::vector<PendingLaunch> pending;
+  std::vector<cudaEvent_t> event_pool;
+
+  ~mfd_handle() {
+    if (st) cudaStreamSynchronize(st);
+    for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+    if (g_factor) cudaGraphExecDestroy(g_factor);
+    for (auto& kv : g_solve) cudaGraphExecDestroy(kv.second);
+    for (void* p : {d_panel, d_upool, d_diag, d_X, d_V, d_S})
+      if (p) cudaFree(p);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+namespace {
+
+int small_front_max(const mfd_handle* h) {
+  int lim = h->fp32 ? 224 : 160;
+  if (h->opt.small_front_max > 0) lim = std::min(lim, h->opt.small_front_max);
+  return lim;
+}
+
+int32_t push_list(mfd_handle* h, const std::vector<int32_t>& ids) {
+  int32_t off = (int32_t)h->h_lists.size();
+  h->h_lists.insert(h->h_lists.end(), ids.begin(), ids.end());
+  return off;
+}
+
+// ---- plan construction --------------------------------------------------------
+int build_plan(mfd_handle* h) {
+  const int nsys = (int)h->sys.size();
+  h->col_base.assign(nsys + 1, 0);
+  h->a_base.assign(nsys + 1, 0);
+  h->front_base.assign(nsys + 1, 0);
+  for (int s = 0; s < nsys; ++s) {
+    h->col_base[s + 1] = h->col_base[s] + h->sys[s].n;
+    h->a_base[s + 1] = h->a_base[s] + h->sys[s].nnz;
+    h->front_base[s + 1] = h->front_base[s] + h->sys[s].num_node;
+  }
+  h->n_total = h->col_base[nsys];
+  h->nnz_total = h->a_base[nsys];
+  h->num_front = h->front_base[nsys];
+  if (h->n_total >= INT32_MAX || h->nnz_total >= INT32_MAX) return fail(MFD_E_ARG, "system too large for int32 indices");
+  const int32_t nfr = h->num_front;
+  h->fronts.assign(nfr, HostFront{});
+  std::vector<int32_t> lrow_glob;
+  h->h_lrow_off.assign(nfr + 1, 0);
+  h->h_a_beg.assign(nfr + 1, 0);
+  h->cost = h->nonzero = 0;
+  for (int s = 0; s < nsys; ++s) {
+    const Symbolic& S = h->sys[s];
+    for (int node = 0; node < S.num_node; ++node) {
+      int32_t g = h->front_base[s] + node;
+      HostFront& fr = h->fronts[g];
+      fr.nc = S.node_ptr[node + 1] - S.node_ptr[node];
+      fr.nr = S.lrow_ptr[node + 1] - S.lrow_ptr[node];
+      fr.first = (int32_t)(h->col_base[s] + S.node_ptr[node] - 1);
+      fr.parent = S.parent[node] > 0 ? h->front_base[s] + S.parent[node] - 1 : -1;
+      fr.sys = s;
+      fr.node = node;
+      h->h_lrow_off[g] = (int32_t)lrow_glob.size();
+      for (int32_t k = S.lrow_ptr[node] - 1; k < S.lrow_ptr[node + 1] - 1; ++k)
+        lrow_glob.push_back((int32_t)(h->col_base[s] + S.lrow[k] - 1));
+      h->h_a_beg[g] = (int32_t)(h->a_base[s] + S.acol_ptr[S.node_ptr[node] - 1] - 1);
+      for (int64_t k = fr.nr + 1; k <= fr.nr + fr.nc; ++k) {
+        h->cost += k * k;
+        h->nonzero += k;
+      }
+    }
+  }
+  h->h_lrow_off[nfr] = (int32_t)lrow_glob.size();
+  h->h_a_beg[nfr] = (int32_t)h->nnz_total;
+  // children lists (ascending node order == the reference's tree_child order)
+  std::vector<int32_t> cnt(nfr, 0);
+  for (int32_t g = 0; g < nfr; ++g)
+    if (h->fronts[g].parent >= 0) cnt[h->fronts[g].parent]++;
+  h->h_child_ptr.assign(nfr + 1, 0);
+  for (int32_t g = 0; g < nfr; ++g) h->h_child_ptr[g + 1] = h->h_child_ptr[g] + cnt[g];
+  h->h_child.assign(h->h_child_ptr[nfr], 0);
+  {
+    std::vector<int32_t> fill(h->h_child_ptr.begin(), h->h_child_ptr.end() - 1);
+    for (int32_t g = 0; g < nfr; ++g)
+      if (h->fronts[g].parent >= 0) h->h_child[fill[h->fronts[g].parent]++] = g;
+  }
+  // levels: height above the leaves (children precede parents in the numbering)
+  int32_t nlev = 0;
+  for (int32_t g = 0; g < nfr; ++g) {
+    HostFront& fr = h->fronts[g];
+    int lv = 0;
+    for (int32_t t = h->h_child_ptr[g]; t < h->h_child_ptr[g + 1]; ++t)
+      lv = std::max(lv, h->fronts[h->h_child[t]].level + 1);
+    fr.level = lv;
+    nlev = std::max(nlev, lv + 1);
+  }
+  // panel offsets, solve vector offsets, large-front solve scratch
+  const int sfm = small_front_max(h);
+  h->panel_elems = h->v_elems = h->s_elems = 0;
+  h->max_nf = 0;
+  for (int32_t g = 0; g < nfr; ++g) {
+    HostFront& fr = h->fronts[g];
+    int nf = fr.nc + fr.nr;
+    h->max_nf = std::max(h->max_nf, nf);
+    fr.panel_off = h->panel_elems;
+    h->panel_elems += align_up((int64_t)nf * fr.nc);
+    fr.v_off = h->v_elems;
+    h->v_elems += nf;
+    fr.s_off = h->s_elems;
+    if (nf > sfm) h->s_elems += (int64_t)((nf + kSolveRows - 1) / kSolveRows) * kPanelB;
+  }
+  // update pool: static first-fit plan over level lifetimes
+  {
+    std::vector<std::vector<int32_t>> by_level(nlev);
+    for (int32_t g = 0; g < nfr; ++g) by_level[h->fronts[g].level].push_back(g);
+    FirstFit ff;
+    for (int l = 0; l < nlev; ++l) {
+      for (int32_t g : by_level[l]) {
+        int64_t nr = h->fronts[g].nr;
+        h->fronts[g].u_off = ff.alloc(nr * nr);
+      }
+      for (int32_t g : by_level[l])
+        for (int32_t t = h->h_child_ptr[g]; t < h->h_child_ptr[g + 1]; ++t) {
+          const HostFront& c = h->fronts[h->h_child[t]];
+          ff.release(c.u_off, (int64_t)c.nr * c.nr);
+        }
+    }
+    h->upool_elems = std::max<int64_t>(ff.top, kAlign);
+  }
+  // level launch lists
+  h->small_bins = h->fp32 ? std::vector<int>{32, 64, 96, 128, 160, 192, 224} : std::vector<int>{32, 64, 96, 128, 160};
+  while (!h->small_bins.empty() && h->small_bins.back() > sfm) h->small_bins.pop_back();
+  if (h->small_bins.empty() || h->small_bins.back() < sfm) h->small_bins.push_back(sfm);
+  h->levels.assign(nlev, LevelPlan{});
+  h->h_lists.clear();
+  h->max_large_count = 0;
+  std::vector<std::vector<int32_t>> lev_fronts(nlev);
+  for (int32_t g = 0; g < nfr; ++g) lev_fronts[h->fronts[g].level].push_back(g);
+  for (int l = 0; l < nlev; ++l) {
+    LevelPlan& L = h->levels[l];
+    std::vector<std::vector<int32_t>> bins(h->small_bins.size());
+    std::vector<int32_t> large;
+    for (int32_t g : lev_fronts[l]) {
+      int nf = h->fronts[g].nc + h->fronts[g].nr;
+      if (nf <= sfm) {
+        size_t b = 0;
+        while (h->small_bins[b] < nf) ++b;
+        bins[b].push_back(g);
+      } else {
+        large.push_back(g);
+      }
+    }
+    for (size_t b = 0; b < bins.size(); ++b) {
+      if (bins[b].empty()) continue;
+      LaunchList ll;
+      ll.off = push_list(h, bins[b]);
+      ll.count = (int32_t)bins[b].size();
+      ll.param = h->small_bins[b];
+      L.small.push_back(ll);
+    }
+    if (large.empty()) continue;
+    std::stable_sort(large.begin(), large.end(),
+                     [&](int32_t a, int32_t b) { return h->fronts[a].nc > h->fronts[b].nc; });
+    L.large.off = push_list(h, large);
+    L.large.count = (int32_t)large.size();
+    h->max_large_count = std::max(h->max_large_count, L.large.count);
+    int max_entries = 0;
+    int64_t max_elems = 0;
+    int max_nc = 0;
+    for (int32_t g : large) {
+      const HostFront& fr = h->fronts[g];
+      int nf = fr.nc + fr.nr;
+      max_entries = std::max(max_entries, h->h_a_beg[g + 1] - h->h_a_beg[g]);
+      max_elems = std::max(max_elems, std::max<int64_t>((int64_t)nf * fr.nc, (int64_t)fr.nr * fr.nr));
+      max_nc = std::max(max_nc, fr.nc);
+      L.large_max_nf = std::max(L.large_max_nf, nf);
+    }
+    L.large.param = max_entries;
+    L.large.param2 = max_nc;
+    L.large_zero_elems = max_elems;
+    // extend-add by child rank
+    for (int rank = 0;; ++rank) {
+      std::vector<int32_t> kids;
+      int max_nr = 0;
+      for (int32_t g : large) {
+        int32_t t = h->h_child_ptr[g] + rank;
+        if (t < h->h_child_ptr[g + 1]) {
+          kids.push_back(h->h_child[t]);
+          max_nr = std::max(max_nr, h->fronts[h->h_child[t]].nr);
+        }
+      }
+      if (kids.empty()) break;
+      LaunchList ll;
+      ll.off = push_list(h, kids);
+      ll.count = (int32_t)kids.size();
+      ll.param = max_nr;
+      L.ext_add.push_back(ll);
+    }
+    // panel steps: prefix of the nc-sorted list
+    int steps = (max_nc + kPanelB - 1) / kPanelB;
+    for (int s = 0; s < steps; ++s) {
+      LaunchList ll;
+      ll.off = L.large.off;
+      int cntf = 0, rows = 1, tiles = 1;
+      for (int32_t g : large) {
+        const HostFront& fr = h->fronts[g];
+        if (fr.nc <= s * kPanelB) break;
+        ++cntf;
+        int w = std::min(kPanelB, fr.nc - s * kPanelB);
+        int nrem = fr.nc + fr.nr - s * kPanelB - w;
+        rows = std::max(rows, (nrem + kPanelRows - 1) / kPanelRows);
+        int T = (nrem + kTile - 1) / kTile;
+        tiles = std::max(tiles, T * (T + 1) / 2);
+      }
+      ll.count = cntf;
+      ll.param = rows;
+      ll.param2 = tiles;
+      L.steps.push_back(ll);
+    }
+  }
+  return MFD_OK;
+}
+
+int upload_plan(mfd_handle* h) {
+  cudaStream_t st = h->st;
+  const int32_t nfr = h->num_front;
+  std::vector<int32_t> nc(nfr), nr(nfr), first(nfr), parent(nfr);
+  std::vector<int64_t> poff(nfr), uoff(nfr), voff(nfr), soff(nfr);
+  for (int32_t g = 0; g < nfr; ++g) {
+    const HostFront& f = h->fronts[g];
+    nc[g] = f.nc; nr[g] = f.nr; first[g] = f.first; parent[g] = f.parent;
+    poff[g] = f.panel_off; uoff[g] = f.u_off; voff[g] = f.v_off; soff[g] = f.s_off;
+  }
+  std::vector<int32_t> lrow_glob;
+  lrow_glob.reserve(h->h_lrow_off[nfr]);
+  for (int s = 0; s < (int)h->sys.size(); ++s)
+    for (int32_t v : h->sys[s].lrow) lrow_glob.push_back((int32_t)(h->col_base[s] + v - 1));
+  CK(h->d_nc.upload(nc, st));
+  CK(h->d_nr.upload(nr, st));
+  CK(h->d_first.upload(first, st));
+  CK(h->d_parent.upload(parent, st));
+  CK(h->d_child_ptr.upload(h->h_child_ptr, st));
+  CK(h->d_child.upload(h->h_child, st));
+  CK(h->d_lrow_off.upload(h->h_lrow_off, st));
+  CK(h->d_lrow.upload(lrow_glob, st));
+  CK(h->d_local.alloc(std::max<size_t>(lrow_glob.size(), 1)));
+  CK(h->d_a_beg.upload(h->h_a_beg, st));
+  CK(h->d_panel_off.upload(poff, st));
+  CK(h->d_u_off.upload(uoff, st));
+  CK(h->d_v_off.upload(voff, st));
+  CK(h->d_s_off.upload(soff, st));
+  CK(h->d_lists.upload(h->h_lists, st));
+  CK(h->d_a_src.alloc(h->nnz_total));
+  CK(h->d_a_pos.alloc(h->nnz_total));
+  CK(h->d_sidx.alloc(h->nnz_total));
+  CK(h->d_info.alloc(1));
+  DevFronts& F = h->F;
+  F.nc = h->d_nc.p; F.nr = h->d_nr.p; F.first = h->d_first.p; F.parent = h->d_parent.p;
+  F.child_ptr = h->d_child_ptr.p; F.child = h->d_child.p; F.panel_off = h->d_panel_off.p; F.u_off = h->d_u_off.p;
+  F.lrow_off = h->d_lrow_off.p; F.lrow = h->d_lrow.p; F.local = h->d_local.p; F.a_beg = h->d_a_beg.p;
+  F.a_src = h->d_a_src.p; F.a_pos = h->d_a_pos.p; F.v_off = h->d_v_off.p; F.s_off = h->d_s_off.p;
+
+  // permuted global A structure, value sources, front of every column
+  std::vector<int32_t> acol(h->n_total + 1), arow(h->nnz_total), src(h->nnz_total), colf(h->n_total),
+      perm(h->n_total);
+  for (int s = 0; s < (int)h->sys.size(); ++s) {
+    const Symbolic& S = h->sys[s];
+    for (int32_t j = 0; j < S.n; ++j) {
+      acol[h->col_base[s] + j] = (int32_t)(h->a_base[s] + S.acol_ptr[j] - 1);
+      perm[h->col_base[s] + j] = (int32_t)(h->col_base[s] + S.perm[j] - 1);
+    }
+    for (int32_t k = 0; k < S.nnz; ++k) {
+      arow[h->a_base[s] + k] = (int32_t)(h->col_base[s] + S.arow[k] - 1);
+      src[h->a_base[s] + k] = (int32_t)(h->a_base[s] + S.ccs_perm[k] - 1);
+    }
+    for (int node = 0; node < S.num_node; ++node)
+      for (int32_t j = S.node_ptr[node] - 1; j < S.node_ptr[node + 1] - 1; ++j)
+        colf[h->col_base[s] + j] = h->front_base[s] + node;
+  }
+  acol[h->n_total] = (int32_t)h->nnz_total;
+  CK(h->d_perm.upload(perm, st));
+  DBuf<int32_t> d_acol, d_arow, d_src, d_colf;
+  CK(d_acol.upload(acol, st));
+  CK(d_arow.upload(arow, st));
+  CK(d_src.upload(src, st));
+  CK(d_colf.upload(colf, st));
+  launch_local_index(F, h->d_local.p, nfr, st);
+  launch_assembly_map(F, d_colf.p, d_acol.p, d_arow.p, d_src.p, h->d_sidx.p, h->d_a_src.p, h->d_a_pos.p,
+                      (int)h->n_total, st);
+  CK(cudaGetLastError());
+
+  // block-local index per system (export for parity)
+  const int nb = std::max(1, h->opt.nb);
+  h->bli_node_ptr.assign(h->sys.size(), {});
+  h->bli_block_ptr.assign(h->sys.size(), {});
+  h->bli_pnum.assign(h->sys.size(), {});
+  h->bli_cnum.assign(h->sys.size(), {});
+  h->bli_off.assign(h->sys.size(), {});
+  h->bli_val.assign(h->sys.size(), {});
+  {
+    std::vector<int32_t> all(nfr);
+    for (int32_t g = 0; g < nfr; ++g) all[g] = g;
+    DBuf<int32_t> d_all, d_groups;
+    CK(d_all.upload(all, st));
+    CK(d_groups.alloc(nfr));
+    launch_bli_count(F, d_all.p, nfr, nb, d_groups.p, st);
+    std::vector<int32_t> groups(nfr);
+    CK(cudaMemcpyAsync(groups.data(), d_groups.p, sizeof(int32_t) * nfr, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // group / index bases relative to each system (1-based group ids)
+    std::vector<int32_t> gbase(nfr), ibase(nfr);
+    int64_t total_groups = 0;
+    for (int s = 0; s < (int)h->sys.size(); ++s) {
+      int32_t gacc = 0;
+      auto& np = h->bli_node_ptr[s];
+      np.assign(h->sys[s].num_node + 1, 1);
+      for (int node = 0; node < h->sys[s].num_node; ++node) {
+        int32_t g = h->front_base[s] + node;
+        gbase[g] = (int32_t)(total_groups + gacc + 1);
+        ibase[g] = h->sys[s].lrow_ptr[node] - 1;
+        gacc += groups[g];
+        np[node + 1] = 1 + gacc;
+      }
+      total_groups += gacc;
+    }
+    DBuf<int32_t> d_gbase, d_ibase, d_bptr, d_pnum, d_cnum, d_off, d_reb;
+    CK(d_gbase.upload(gbase, st));
+    CK(d_ibase.upload(ibase, st));
+    CK(d_bptr.alloc(total_groups));
+    CK(d_pnum.alloc(total_groups));
+    CK(d_cnum.alloc(total_groups));
+    CK(d_off.alloc(total_groups));
+    // rebuilt values are written at the system-relative index: use a global buffer with per-system offsets
+    CK(d_reb.alloc(std::max<size_t>(h->h_lrow_off[nfr], 1)));
+    // rebuild index base = global lrow offset for the value array, system-relative for block_ptr
+    std::vector<int32_t> vbase(nfr);
+    for (int32_t g = 0; g < nfr; ++g) vbase[g] = h->h_lrow_off[g];
+    DBuf<int32_t> d_vbase;
+    CK(d_vbase.upload(vbase, st));
+    // block_ptr needs system-relative bases; rebuilt needs global bases: run with system-relative bases for
+    // block_ptr and fix the rebuilt values from local on the host side (same formula), cheaper than two passes.
+    launch_bli_fill(F, d_all.p, nfr, nb, d_gbase.p, d_ibase.p, d_bptr.p, d_pnum.p, d_cnum.p, d_off.p, d_reb.p, st);
+    CK(cudaGetLastError());
+    std::vector<int32_t> bptr(total_groups), pn(total_groups), cn(total_groups), of(total_groups);
+    std::vector<int32_t> local(h->h_lrow_off[nfr]), sidx(h->nnz_total);
+    if (total_groups) {
+      CK(cudaMemcpyAsync(bptr.data(), d_bptr.p, sizeof(int32_t) * total_groups, cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(pn.data(), d_pnum.p, sizeof(int32_t) * total_groups, cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(cn.data(), d_cnum.p, sizeof(int32_t) * total_groups, cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(of.data(), d_off.p, sizeof(int32_t) * total_groups, cudaMemcpyDeviceToHost, st));
+    }
+    if (!local.empty())
+      CK(cudaMemcpyAsync(local.data(), h->d_local.p, sizeof(int32_t) * local.size(), cudaMemcpyDeviceToHost, st));
+    if (!sidx.empty())
+      CK(cudaMemcpyAsync(sidx.data(), h->d_sidx.p, sizeof(int32_t) * sidx.size(), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // every index the numeric kernels will follow must point inside its front
+    for (int32_t v : local)
+      if (v <= 0) return fail(MFD_E_ARG, "inconsistent symbolic structure (child row not in parent front)");
+    for (int32_t v : sidx)
+      if (v <= 0) return fail(MFD_E_ARG, "inconsistent symbolic structure (A entry outside its front)");
+    // the rebuilt (mod nb) local values: k_bli_fill wrote them at system-relative offsets of d_reb, which
+    // collide across systems; derive them per system from the device-built local index instead.
+    h->local_sys.assign(h->sys.size(), {});
+    h->sidx_sys.assign(h->sys.size(), {});
+    int64_t goff = 0;
+    for (int s = 0; s < (int)h->sys.size(); ++s) {
+      int32_t ng = h->bli_node_ptr[s].back() - 1;
+      h->bli_block_ptr[s].assign(bptr.begin() + goff, bptr.begin() + goff + ng);
+      h->bli_block_ptr[s].push_back((int32_t)h->sys[s].lrow.size() + 1);
+      h->bli_pnum[s].assign(pn.begin() + goff, pn.begin() + goff + ng);
+      h->bli_cnum[s].assign(cn.begin() + goff, cn.begin() + goff + ng);
+      h->bli_off[s].assign(of.begin() + goff, of.begin() + goff + ng);
+      goff += ng;
+      int32_t lo = h->h_lrow_off[h->front_base[s]], hi = h->h_lrow_off[h->front_base[s + 1]];
+      h->local_sys[s].assign(local.begin() + lo, local.begin() + hi);
+      h->bli_val[s].resize(h->local_sys[s].size());
+      for (size_t i = 0; i < h->local_sys[s].size(); ++i) h->bli_val[s][i] = (h->local_sys[s][i] - 1) % nb + 1;
+      h->sidx_sys[s].assign(sidx.begin() + h->a_base[s], sidx.begin() + h->a_base[s + 1]);
+    }
+  }
+
+  // permuted full CSR (both triangles) for residuals
+  {
+    std::vector<int64_t> rp(h->n_total + 1, 0);
+    for (int64_t j = 0; j < h->n_total; ++j)
+      for (int32_t k = acol[j]; k < acol[j + 1]; ++k) {
+        rp[arow[k] + 1]++;
+        if (arow[k] != j) rp[j + 1]++;
+      }
+    for (int64_t i = 0; i < h->n_total; ++i) rp[i + 1] += rp[i];
+    std::vector<int32_t> cols(rp.back()), srcs(rp.back());
+    std::vector<int64_t> fill(rp.begin(), rp.end() - 1);
+    for (int64_t j = 0; j < h->n_total; ++j)
+      for (int32_t k = acol[j]; k < acol[j + 1]; ++k) {
+        int32_t r = arow[k];
+        cols[fill[r]] = (int32_t)j; srcs[fill[r]++] = src[k];
+        if (r != j) { cols[fill[j]] = r; srcs[fill[j]++] = src[k]; }
+      }
+    CK(h->d_csr_ptr.upload(rp, st));
+    CK(h->d_csr_col.upload(cols, st));
+    CK(h->d_csr_src.upload(srcs, st));
+    CK(h->d_csr_val.alloc(cols.size()));
+  }
+  CK(cudaStreamSynchronize(st));
+
+  // numeric storage
+  size_t esz = h->fp32 ? sizeof(float) : sizeof(double);
+  CK(cudaMalloc(&h->d_panel, std::max<int64_t>(h->panel_elems, 1) * esz));
+  CK(cudaMalloc(&h->d_upool, std::max<int64_t>(h->upool_elems, 1) * esz));
+  CK(cudaMalloc(&h->d_diag, (size_t)std::max(1, h->max_large_count) * kPanelB * kPanelB * esz));
+  CK(h->d_a.alloc(h->nnz_total));
+  CK(h->d_norms.alloc(8));
+  return MFD_OK;
+}
+
+int ensure_rhs(mfd_handle* h, int nrhs) {
+  if (nrhs <= h->nrhs_cap) return MFD_OK;
+  for (auto& kv : h->g_solve) cudaGraphExecDestroy(kv.second);
+  h->g_solve.clear();
+  size_t esz = h->fp32 ? sizeof(float) : sizeof(double);
+  for (void** p : {&h->d_X, &h->d_V, &h->d_S})
+    if (*p) { cudaFree(*p); *p = nullptr; }
+  CK(cudaMalloc(&h->d_X, (size_t)std::max<int64_t>(h->n_total, 1) * nrhs * esz));
+  CK(cudaMalloc(&h->d_V, (size_t)std::max<int64_t>(h->v_elems, 1) * nrhs * esz));
+  CK(cudaMalloc(&h->d_S, (size_t)std::max<int64_t>(h->s_elems, 1) * nrhs * esz));
+  CK(h->d_b.alloc((size_t)h->n_total * nrhs));
+  CK(h->d_xp.alloc((size_t)h->n_total * nrhs));
+  CK(h->d_bp.alloc((size_t)h->n_total * nrhs));
+  CK(h->d_r.alloc((size_t)h->n_total * nrhs));
+  h->nrhs_cap = nrhs;
+  return MFD_OK;
+}
+
+// ---- per-launch profiling ----------------------------------------------------------
+cudaEvent_t take_event(mfd_handle* h, size_t idx) {
+  while (h->event_pool.size() <= idx) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    h->event_pool.push_back(e);
+  }
+  return h->event_pool[idx];
+}
+
+// Runs `launch` and, when profiling, brackets it with events on the stream.
+template <typename Fn>
+void record(mfd_handle* h, cudaStream_t st, int kind, double flops, double bytes, Fn&& launch) {
+  if (!h->profiling) {
+    launch();
+    return;
+  }
+  size_t i = h->pending.size() * 2;
+  cudaEvent_t a = take_event(h, i), b = take_event(h, i + 1);
+  cudaEventRecord(a, st);
+  launch();
+  cudaEventRecord(b, st);
+  h->pending.push_back({kind, flops, bytes, a, b});
+}
+
+void collect_profile(mfd_handle* h) {
+  for (auto& p : h->pending) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    mfd_kernel_profile& k = h->prof[p.kind];
+    k.launches += 1;
+    k.ms += ms;
+    k.flops += p.flops;
+    k.bytes += p.bytes;
+  }
+  h->pending.clear();
+}
+
+// algorithmic work of one front's fused factorization (w = element size)
+void small_work(const mfd_handle* h, int32_t g, double w, double& flops, double& bytes) {
+  const HostFront& f = h->fronts[g];
+  double nc = f.nc, nr = f.nr, nf = nc + nr;
+  for (int64_t k = f.nr + 1; k <= f.nr + f.nc; ++k) flops += (double)k * (double)k;
+  bytes += w * (nf * nc - nc * (nc - 1) / 2 + nr * (nr + 1) / 2) + 12.0 * (h->h_a_beg[g + 1] - h->h_a_beg[g]);
+  for (int32_t t = h->h_child_ptr[g]; t < h->h_child_ptr[g + 1]; ++t) {
+    double c = h->fronts[h->h_child[t]].nr;
+    bytes += w * c * (c + 1) / 2 + 4.0 * c;
+  }
+}
+
+// ---- launch sequences ------------------------------------------------------------
+template <typename T>
+int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
+  int64_t n = 0;
+  const DevFronts& F = h->F;
+  T* panel = static_cast<T*>(h->d_panel);
+  T* upool = static_cast<T*>(h->d_upool);
+  T* diag = static_cast<T*>(h->d_diag);
+  const int32_t* lists = h->d_lists.p;
+  const double* a = h->d_a.p;
+  const double w = sizeof(T);
+  const bool prof = h->profiling;
+  const int32_t* hl = h->h_lists.data();
+  launch_fill_int(h->d_info.p, INT_MAX, 1, st);
+  ++n;
+  const int kind = h->opt.reserved[0] == 1 ? 1 : 0;   // 0: DMMA trailing update (FP64), 1: FFMA tiles
+  for (const LevelPlan& L : h->levels) {
+    for (const LaunchList& s : L.small) {
+      double fl = 0, by = 0;
+      if (prof)
+        for (int i = 0; i < s.count; ++i) small_work(h, hl[s.off + i], w, fl, by);
+      record(h, st, MFD_K_SMALL_FRONT, fl, by,
+             [&] { launch_small_fronts<T>(F, lists + s.off, s.count, s.param, a, panel, upool, h->d_info.p, st); });
+      ++n;
+    }
+    if (L.large.count == 0) continue;
+    double zb = 0, ab = 0;
+    if (prof)
+      for (int i = 0; i < L.large.count; ++i) {
+        const HostFront& f = h->fronts[hl[L.large.off + i]];
+        zb += w * ((double)(f.nc + f.nr) * f.nc + (double)f.nr * f.nr);
+        ab += 12.0 * (h->h_a_beg[hl[L.large.off + i] + 1] - h->h_a_beg[hl[L.large.off + i]]);
+      }
+    record(h, st, MFD_K_ZERO, 0, zb,
+           [&] { launch_zero_large<T>(F, lists + L.large.off, L.large.count, L.large_zero_elems, panel, upool, st); });
+    record(h, st, MFD_K_ASSEMBLE, 0, ab,
+           [&] { launch_assemble_large<T>(F, lists + L.large.off, L.large.count, L.large.param, a, panel, st); });
+    n += 2;
+    for (const LaunchList& e : L.ext_add) {
+      double fl = 0, by = 0;
+      if (prof)
+        for (int i = 0; i < e.count; ++i) {
+          double c = h->fronts[hl[e.off + i]].nr;
+          fl += c * (c + 1) / 2;
+          by += 3 * w * c * (c + 1) / 2 + 4.0 * c;
+        }
+      record(h, st, MFD_K_EXTEND_ADD, fl, by,
+             [&] { launch_extend_add<T>(F, lists + e.off, e.count, e.param, panel, upool, st); });
+      ++n;
+    }
+    for (size_t s = 0; s < L.steps.size(); ++s) {
+      const LaunchList& p = L.steps[s];
+      double pf = 0, pb = 0, uf = 0, ub = 0;
+      if (prof)
+        for (int i = 0; i < p.count; ++i) {
+          const HostFront& f = h->fronts[hl[p.off + i]];
+          double c0 = (double)s * kPanelB, wd = std::min<double>(kPanelB, f.nc - c0);
+          double nrem = f.nc + f.nr - c0 - wd;
+          pf += wd * wd * wd / 3 + nrem * wd * wd;
+          pb += w * (wd * wd / 2 + nrem * wd) * 2;
+          uf += 2.0 * wd * nrem * (nrem + 1) / 2;
+          ub += w * (2.0 * nrem * (nrem + 1) / 2 + 2.0 * nrem * wd);
+        }
+      record(h, st, MFD_K_PANEL, pf, pb,
+             [&] { launch_panel<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, h->d_info.p, st); });
+      record(h, st, MFD_K_UPDATE, uf, ub, [&] {
+        launch_update<T>(F, lists + p.off, p.count, (int)s, p.param2, panel, upool, diag, kind, st);
+      });
+      n += 2;
+    }
+  }
+  // values of the permuted full matrix for residuals
+  record(h, st, MFD_K_OTHER, 0, 0, [&] {
+    launch_gather_values(a, h->d_csr_src.p, h->d_csr_val.p, (int64_t)h->d_csr_val.n, st);
+    launch_row_abs_max(h->d_csr_ptr.p, h->d_csr_val.p, h->n_total, h->d_norms.p + 7, st);
+  });
+  n += 2;
+  return n;
+}
+
+template <typename T>
+int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
+  int64_t n = 0;
+  const DevFronts& F = h->F;
+  const T* panel = static_cast<const T*>(h->d_panel);
+  T* X = static_cast<T*>(h->d_X);
+  T* V = static_cast<T*>(h->d_V);
+  T* S = static_cast<T*>(h->d_S);
+  const int32_t* lists = h->d_lists.p;
+  const int64_t ldx = h->n_total;
+  const double w = sizeof(T);
+  const bool prof = h->profiling;
+  const int32_t* hl = h->h_lists.data();
+  // algorithmic work of one sweep over a list: read the panel once, 2 flops per entry per RHS
+  auto work = [&](const LaunchList& l, double& fl, double& by) {
+    if (!prof) return;
+    for (int i = 0; i < l.count; ++i) {
+      const HostFront& f = h->fronts[hl[l.off + i]];
+      double e = (double)(f.nc + f.nr) * f.nc - (double)f.nc * (f.nc - 1) / 2;
+      fl += 2.0 * e * nrhs;
+      by += w * e + w * nrhs * (2.0 * (f.nc + f.nr) + f.nr);
+    }
+  };
+  for (const LevelPlan& L : h->levels) {
+    for (const LaunchList& s : L.small) {
+      double fl = 0, by = 0;
+      work(s, fl, by);
+      record(h, st, MFD_K_SOLVE_SMALL, fl, by,
+             [&] { launch_fwd_small<T>(F, lists + s.off, s.count, s.param, panel, X, ldx, V, nrhs, st); });
+      ++n;
+    }
+    if (L.large.count) {
+      double fl = 0, by = 0;
+      work(L.large, fl, by);
+      record(h, st, MFD_K_SOLVE_LARGE, fl, by, [&] {
+        launch_fwd_large<T>(F, lists + L.large.off, L.large.count, L.large.param2, L.large_max_nf, panel, X, ldx, V,
+                            nrhs, st, &n);
+      });
+    }
+  }
+  for (auto it = h->levels.rbegin(); it != h->levels.rend(); ++it) {
+    const LevelPlan& L = *it;
+    if (L.large.count) {
+      double fl = 0, by = 0;
+      work(L.large, fl, by);
+      record(h, st, MFD_K_SOLVE_LARGE, fl, by, [&] {
+        launch_bwd_large<T>(F, lists + L.large.off, L.large.count, L.large.param2, L.large_max_nf, panel, X, ldx, V,
+                            S, nrhs, st, &n);
+      });
+    }
+    for (const LaunchList& s : L.small) {
+      double fl = 0, by = 0;
+      work(s, fl, by);
+      record(h, st, MFD_K_SOLVE_SMALL, fl, by,
+             [&] { launch_bwd_small<T>(F, lists + s.off, s.count, s.param, panel, X, ldx, nrhs, st); });
+      ++n;
+    }
+  }
+  return n;
+}
+
+template <typename Fn>
+int run_graph(mfd_handle* h, cudaGraphExec_t* exec, Fn&& fn) {
+  if (!h->opt.use_graph || h->profiling) {
+    fn(h->st);
+    CK(cudaGetLastError());
+    return MFD_OK;
+  }
+  if (!*exec) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    fn(h->st);
+    cudaError_t e = cudaStreamEndCapture(h->st, &g);
+    if (e != cudaSuccess) return fail(MFD_E_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(MFD_E_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+  }
+  CK(cudaGraphLaunch(*exec, h->st));
+  return MFD_OK;
+}
+
+bool is_device_ptr(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+int do_factorize(mfd_handle* h, const double* a) {
+  if (!a) return fail(MFD_E_ARG, "null values");
+  CK(cudaSetDevice(h->device));
+  cudaMemcpyKind kind = is_device_ptr(a) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CK(cudaMemcpyAsync(h->d_a.p, a, sizeof(double) * h->nnz_total, kind, h->st));
+  CK(cudaEventRecord(h->ev0, h->st));
+  int rc = h->fp32 ? run_graph(h, &h->g_factor, [&](cudaStream_t s) { h->launches_factor = enqueue_factor<float>(h, s); })
+                   : run_graph(h, &h->g_factor, [&](cudaStream_t s) { h->launches_factor = enqueue_factor<double>(h, s); });
+  if (rc) return rc;
+  CK(cudaEventRecord(h->ev1, h->st));
+  int32_t info = 0;
+  double anorm = 0;
+  CK(cudaMemcpyAsync(&info, h->d_info.p, sizeof(int32_t), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaMemcpyAsync(&anorm, h->d_norms.p + 7, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  collect_profile(h);
+  h->factor_ms = ms;
+  h->anorm = anorm;
+  h->time_info[6] = ms * 1e-3;
+  h->factored = true;
+  if (info != INT_MAX) {
+    // map the global permuted column to the system-relative 1-based column
+    int64_t col = info - 1;
+    int s = (int)(std::upper_bound(h->col_base.begin(), h->col_base.end(), col) - h->col_base.begin()) - 1;
+    h->factored = false;
+    g_err = "matrix is not positive definite (system " + std::to_string(s) + ")";
+    return (int)(col - h->col_base[s] + 1);
+  }
+  return MFD_OK;
+}
+
+template <typename T>
+int solve_core(mfd_handle* h, int nrhs) {
+  auto it = h->g_solve.find(nrhs);
+  cudaGraphExec_t exec = it == h->g_solve.end() ? nullptr : it->second;
+  int rc = run_graph(h, &exec, [&](cudaStream_t s) { h->launches_solve = enqueue_solve_core<T>(h, nrhs, s); });
+  if (exec) h->g_solve[nrhs] = exec;
+  return rc;
+}
+
+int residual_report(mfd_handle* h, const double* xp, const double* bp, mfd_report* rep, double* bwd) {
+  launch_residual(h->d_csr_ptr.p, h->d_csr_col.p, h->d_csr_val.p, xp, bp, h->d_r.p, h->n_total, h->st);
+  launch_norms(h->d_r.p, xp, bp, h->n_total, h->d_norms.p, h->st);
+  double nv[5];
+  CK(cudaMemcpyAsync(nv, h->d_norms.p, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  double denom = h->anorm * nv[1] + nv[2];
+  *bwd = denom > 0 ? nv[0] / denom : nv[0];
+  if (rep) {
+    rep->backward_error = *bwd;
+    rep->residual_ref = nv[4] > 0 ? std::sqrt(nv[3]) / std::sqrt(nv[4]) : std::sqrt(nv[3]);
+  }
+  return MFD_OK;
+}
+
+int do_solve(mfd_handle* h, double* b, int nrhs, int64_t ldb, mfd_report* rep) {
+  if (!h->factored) return fail(MFD_E_STATE, "solve before a successful factorize");
+  if (!b || nrhs < 1 || ldb < h->n_total) return fail(MFD_E_ARG, "bad right-hand side");
+  CK(cudaSetDevice(h->device));
+  int rc = ensure_rhs(h, nrhs);
+  if (rc) return rc;
+  const bool dev = is_device_ptr(b);
+  const int64_t n = h->n_total;
+  cudaStream_t st = h->st;
+  if (ldb == n) {
+    CK(cudaMemcpyAsync(h->d_b.p, b, sizeof(double) * n * nrhs, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  } else {
+    CK(cudaMemcpy2DAsync(h->d_b.p, sizeof(double) * n, b, sizeof(double) * ldb, sizeof(double) * n, nrhs,
+                         dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  }
+  CK(cudaEventRecord(h->ev0, st));
+  int iters = 0;
+  double bwd = 0;
+  bool want_report = rep != nullptr || h->fp32;
+  if (!h->fp32) {
+    launch_permute_in<double>(h->d_b.p, n, h->d_perm.p, static_cast<double*>(h->d_X), n, n, nrhs, st);
+    rc = solve_core<double>(h, nrhs);
+    if (rc) return rc;
+    CK(cudaEventRecord(h->ev1, st));
+    if (want_report) {
+      launch_permute_in<double>(h->d_b.p, n, h->d_perm.p, h->d_bp.p, n, n, 1, st);
+      rc = residual_report(h, static_cast<double*>(h->d_X), h->d_bp.p, rep, &bwd);
+      if (rc) return rc;
+    }
+    launch_permute_out<double>(static_cast<double*>(h->d_X), n, h->d_perm.p, h->d_b.p, n, n, nrhs, st);
+  } else {
+    // FP32 factor + FP64 iterative refinement, one right-hand side at a time
+    bool converged = true;
+    for (int r = 0; r < nrhs; ++r) {
+      double* bcol = h->d_b.p + (int64_t)r * n;
+      launch_permute_in<double>(bcol, n, h->d_perm.p, h->d_bp.p, n, n, 1, st);
+      CK(cudaMemsetAsync(h->d_xp.p, 0, sizeof(double) * n, st));
+      CK(cudaMemcpyAsync(h->d_r.p, h->d_bp.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      int it = 0;
+      const int maxit = h->opt.ir_max_iter > 0 ? h->opt.ir_max_iter : 20;
+      double prev = 1e300;
+      for (; it < maxit; ++it) {
+        launch_to_t<float>(h->d_r.p, static_cast<float*>(h->d_X), n, st);
+        rc = solve_core<float>(h, 1);
+        if (rc) return rc;
+        launch_axpy_from_t<float>(static_cast<float*>(h->d_X), h->d_xp.p, n, st);
+        rc = residual_report(h, h->d_xp.p, h->d_bp.p, rep, &bwd);
+        if (rc) return rc;
+        if (bwd <= h->opt.ir_tol) { ++it; break; }
+        if (bwd > 0.9 * prev && it > 2) { ++it; break; }   // stagnation
+        prev = bwd;
+      }
+      iters = std::max(iters, it);
+      if (bwd > h->opt.ir_tol) converged = false;
+      launch_permute_out<double>(h->d_xp.p, n, h->d_perm.p, bcol, n, n, 1, st);
+    }
+    CK(cudaEventRecord(h->ev1, st));
+    if (!converged) rc = MFD_E_NOCONV;
+  }
+  if (ldb == n) {
+    CK(cudaMemcpyAsync(b, h->d_b.p, sizeof(double) * n * nrhs, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  } else {
+    CK(cudaMemcpy2DAsync(b, sizeof(double) * ldb, h->d_b.p, sizeof(double) * n, sizeof(double) * n, nrhs,
+                         dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  collect_profile(h);
+  h->solve_ms = ms;
+  h->time_info[3] = ms * 1e-3;
+  if (rep) {
+    rep->iterations = iters;
+    rep->converged = bwd <= h->opt.ir_tol;
+    rep->time_ms = ms;
+  }
+  if (rc == MFD_E_NOCONV) g_err = "iterative refinement did not reach the tolerance";
+  return rc;
+}
+
+int create_common(mfd_handle** out, std::vector<Symbolic>&& syms, const mfd_options* opt) {
+  if (!out) return fail(MFD_E_ARG, "null handle pointer");
+  std::unique_ptr<mfd_handle> h(new mfd_handle());
+  mfd_default_options(&h->opt);
+  if (opt) h->opt = *opt;
+  if (h->opt.nb <= 0) h->opt.nb = 10;
+  if (h->opt.ir_tol <= 0) h->opt.ir_tol = 1e-12;
+  h->fp32 = h->opt.precision == MFD_PREC_FP32_IR;
+  h->device = h->opt.device;
+  h->sys = std::move(syms);
+  CK(cudaSetDevice(h->device));
+  CK(prepare_kernels());
+  CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&h->ev0));
+  CK(cudaEventCreate(&h->ev1));
+  int rc = build_plan(h.get());
+  if (rc) return rc;
+  rc = upload_plan(h.get());
+  if (rc) return rc;
+  *out = h.release();
+  return MFD_OK;
+}
+
+int check_symbolic(const mfd_symbolic& s) {
+  if (s.n <= 0 || s.num_node <= 0 || s.nnz <= 0) return -1;
+  if (!s.node_ptr || !s.parent || !s.lrow_ptr || !s.acol_ptr || !s.arow || !s.ccs_perm || !s.perm) return -1;
+  if (s.node_ptr[0] != 1 || s.node_ptr[s.num_node] != s.n + 1) return -1;
+  if (s.lrow_ptr[0] != 1 || s.acol_ptr[0] != 1 || s.acol_ptr[s.n] != s.nnz + 1) return -1;
+  for (int i = 0; i < s.num_node; ++i) {
+    if (s.node_ptr[i + 1] <= s.node_ptr[i] || s.lrow_ptr[i + 1] < s.lrow_ptr[i]) return -1;
+    if (s.parent[i] < 0 || s.parent[i] > s.num_node || (s.parent[i] != 0 && s.parent[i] <= i + 1)) return -1;
+    int last = s.node_ptr[i + 1] - 1;
+    for (int k = s.lrow_ptr[i] - 1; k < s.lrow_ptr[i + 1] - 1; ++k) {
+      if (s.lrow[k] <= last || s.lrow[k] > s.n) return -1;
+      if (k > s.lrow_ptr[i] - 1 && s.lrow[k] <= s.lrow[k - 1]) return -1;
+    }
+  }
+  for (int j = 0; j < s.n; ++j)
+    for (int k = s.acol_ptr[j] - 1; k < s.acol_ptr[j + 1] - 1; ++k) {
+      if (s.arow[k] < j + 1 || s.arow[k] > s.n) return -1;
+      if (s.ccs_perm[k] < 1 || s.ccs_perm[k] > s.nnz) return -1;
+    }
+  for (int i = 0; i < s.n; ++i)
+    if (s.perm[i] < 1 || s.perm[i] > s.n) return -1;
+  return 0;
+}
+
+Symbolic copy_symbolic(const mfd_symbolic& s) {
+  Symbolic o;
+  o.n = s.n; o.nnz = s.nnz; o.num_node = s.num_node;
+  o.node_ptr.assign(s.node_ptr, s.node_ptr + s.num_node + 1);
+  o.parent.assign(s.parent, s.parent + s.num_node);
+  o.lrow_ptr.assign(s.lrow_ptr, s.lrow_ptr + s.num_node + 1);
+  o.lrow.assign(s.lrow, s.lrow + (s.lrow_ptr[s.num_node] - 1));
+  o.acol_ptr.assign(s.acol_ptr, s.acol_ptr + s.n + 1);
+  o.arow.assign(s.arow, s.arow + s.nnz);
+  o.ccs_perm.assign(s.ccs_perm, s.ccs_perm + s.nnz);
+  o.perm.assign(s.perm, s.perm + s.n);
+  return o;
+}
+
+}  // namespace
+
+// ==================================================================================
+// C ABI
+// ==================================================================================
+extern "C" {
+
+#pragma GCC visibility push(default)
+
+void mfd_default_options(mfd_options* opt) {
+  if (!opt) return;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->nb = 10;
+  opt->max_zero = 10;
+  opt->precision = MFD_PREC_FP64;
+  opt->ir_max_iter = 20;
+  opt->ir_tol = 1e-12;
+  opt->use_graph = 1;
+  opt->device = 0;
+}
+
+const char* mfd_last_error(void) { return g_err.c_str(); }
+
+int mfd_create(mfd_handle** h, const mfd_symbolic* sym, const mfd_options* opt) {
+  if (!sym || check_symbolic(*sym)) return fail(MFD_E_ARG, "malformed symbolic input");
+  std::vector<Symbolic> v;
+  v.push_back(copy_symbolic(*sym));
+  return create_common(h, std::move(v), opt);
+}
+
+int mfd_create_batch(mfd_handle** h, int32_t num_systems, const mfd_symbolic* syms, const mfd_options* opt) {
+  if (num_systems <= 0 || !syms) return fail(MFD_E_ARG, "empty batch");
+  std::vector<Symbolic> v;
+  v.reserve(num_systems);
+  for (int i = 0; i < num_systems; ++i) {
+    if (check_symbolic(syms[i])) return fail(MFD_E_ARG, "malformed symbolic input in system " + std::to_string(i));
+    v.push_back(copy_symbolic(syms[i]));
+  }
+  return create_common(h, std::move(v), opt);
+}
+
+int mfd_analyze(mfd_handle** h, int32_t n, const int32_t* ccs_col, const int32_t* ccs_row, const int32_t* order_perm,
+                const mfd_options* opt) {
+  mfd_options o;
+  mfd_default_options(&o);
+  if (opt) o = *opt;
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<Symbolic> v(1);
+  if (analyze(n, ccs_col, ccs_row, order_perm, o.max_zero, v[0])) return fail(MFD_E_ARG, "malformed matrix or ordering");
+  double ta = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  int rc = create_common(h, std::move(v), &o);
+  if (rc == MFD_OK) (*h)->time_info[1] = ta;
+  return rc;
+}
+
+struct mfd_analysis {
+  Symbolic s;
+};
+
+int mfd_symbolic_analyze(mfd_analysis** out, int32_t n, const int32_t* ccs_col, const int32_t* ccs_row,
+                         const int32_t* order_perm, int32_t max_zero) {
+  if (!out) return fail(MFD_E_ARG, "null output");
+  std::unique_ptr<mfd_analysis> a(new mfd_analysis());
+  if (analyze(n, ccs_col, ccs_row, order_perm, max_zero, a->s)) return fail(MFD_E_ARG, "malformed matrix or ordering");
+  *out = a.release();
+  return MFD_OK;
+}
+
+int mfd_symbolic_view(const mfd_analysis* a, mfd_symbolic* v) {
+  if (!a || !v) return fail(MFD_E_ARG, "null argument");
+  const Symbolic& s = a->s;
+  v->n = s.n; v->nnz = s.nnz; v->num_node = s.num_node;
+  v->node_ptr = s.node_ptr.data(); v->parent = s.parent.data(); v->lrow_ptr = s.lrow_ptr.data();
+  v->lrow = s.lrow.data(); v->acol_ptr = s.acol_ptr.data(); v->arow = s.arow.data();
+  v->ccs_perm = s.ccs_perm.data(); v->perm = s.perm.data();
+  return MFD_OK;
+}
+
+int mfd_symbolic_free(mfd_analysis* a) {
+  delete a;
+  return MFD_OK;
+}
+
+int mfd_analyze_batch(mfd_handle** h, int32_t num_systems, const int32_t* n, const int32_t* const* ccs_col,
+                      const int32_t* const* ccs_row, const int32_t* const* order_perm, const mfd_options* opt) {
+  if (num_systems <= 0) return fail(MFD_E_ARG, "empty batch");
+  mfd_options o;
+  mfd_default_options(&o);
+  if (opt) o = *opt;
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<Symbolic> v(num_systems);
+  std::vector<int> rcs(num_systems, 0);
+  unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nt; ++t)
+    th.emplace_back([&, t]() {
+      for (int s = (int)t; s < num_systems; s += (int)nt)
+        rcs[s] = analyze(n[s], ccs_col[s], ccs_row[s], order_perm ? order_perm[s] : nullptr, o.max_zero, v[s]);
+    });
+  for (auto& x : th) x.join();
+  for (int s = 0; s < num_systems; ++s)
+    if (rcs[s]) return fail(MFD_E_ARG, "malformed matrix or ordering in system " + std::to_string(s));
+  double ta = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  int rc = create_common(h, std::move(v), &o);
+  if (rc == MFD_OK) (*h)->time_info[1] = ta;
+  return rc;
+}
+
+int mfd_factorize(mfd_handle* h, const double* a) {
+  if (!h) return fail(MFD_E_ARG, "null handle");
+  return do_factorize(h, a);
+}
+
+int mfd_solve(mfd_handle* h, double* b, int32_t nrhs, int64_t ldb, mfd_report* rep) {
+  if (!h) return fail(MFD_E_ARG, "null handle");
+  return do_solve(h, b, nrhs, ldb, rep);
+}
+
+int mfd_factorize_solve(mfd_handle* h, const double* a, double* b, int32_t nrhs, int64_t ldb, mfd_report* rep) {
+  int rc = mfd_factorize(h, a);
+  if (rc) return rc;
+  return mfd_solve(h, b, nrhs, ldb, rep);
+}
+
+int mfd_get_stats(mfd_handle* h, mfd_stats* st) {
+  if (!h || !st) return fail(MFD_E_ARG, "null argument");
+  std::memset(st, 0, sizeof(*st));
+  st->n = h->n_total;
+  st->nnz_a = h->nnz_total;
+  st->num_front = h->num_front;
+  st->num_level = (int64_t)h->levels.size();
+  st->cost = h->cost;
+  st->nonzero = h->nonzero;
+  size_t esz = h->fp32 ? sizeof(float) : sizeof(double);
+  st->panel_bytes = h->panel_elems * (int64_t)esz;
+  st->update_pool_bytes = h->upool_elems * (int64_t)esz;
+  st->launches_factor = h->launches_factor;
+  st->launches_solve = h->launches_solve;
+  st->max_front = h->max_nf;
+  st->factor_ms = h->factor_ms;
+  st->solve_ms = h->solve_ms;
+  std::memcpy(st->time_info, h->time_info, sizeof(st->time_info));
+  return MFD_OK;
+}
+
+int64_t mfd_get_index(mfd_handle* h, int32_t system, int32_t which, int32_t* out) {
+  if (!h || system < 0 || system >= (int32_t)h->sys.size()) return fail(MFD_E_ARG, "bad system");
+  const std::vector<int32_t>* v = nullptr;
+  switch (which) {
+    case 1: v = &h->local_sys[system]; break;
+    case 2: v = &h->sidx_sys[system]; break;
+    case 3: v = &h->bli_node_ptr[system]; break;
+    case 4: v = &h->bli_block_ptr[system]; break;
+    case 5: v = &h->bli_pnum[system]; break;
+    case 6: v = &h->bli_cnum[system]; break;
+    case 7: v = &h->bli_val[system]; break;
+    case 8: v = &h->bli_off[system]; break;
+    default: return fail(MFD_E_ARG, "bad index id");
+  }
+  if (out && !v->empty()) std::memcpy(out, v->data(), v->size() * sizeof(int32_t));
+  return (int64_t)v->size();
+}
+
+int64_t mfd_get_symbolic(mfd_handle* h, int32_t system, int32_t which, int32_t* out) {
+  if (!h || system < 0 || system >= (int32_t)h->sys.size()) return fail(MFD_E_ARG, "bad system");
+  const Symbolic& S = h->sys[system];
+  const std::vector<int32_t>* v = nullptr;
+  switch (which) {
+    case 1: v = &S.node_ptr; break;
+    case 2: v = &S.parent; break;
+    case 3: v = &S.lrow_ptr; break;
+    case 4: v = &S.lrow; break;
+    case 5: v = &S.acol_ptr; break;
+    case 6: v = &S.arow; break;
+    case 7: v = &S.ccs_perm; break;
+    case 8: v = &S.perm; break;
+    default: return fail(MFD_E_ARG, "bad symbolic id");
+  }
+  if (out && !v->empty()) std::memcpy(out, v->data(), v->size() * sizeof(int32_t));
+  return (int64_t)v->size();
+}
+
+int64_t mfd_get_front_panel(mfd_handle* h, int32_t system, int32_t node, double* out) {
+  if (!h || system < 0 || system >= (int32_t)h->sys.size()) return fail(MFD_E_ARG, "bad system");
+  if (node < 1 || node > h->sys[system].num_node) return fail(MFD_E_ARG, "bad node");
+  const HostFront& f = h->fronts[h->front_base[system] + node - 1];
+  int64_t cnt = (int64_t)(f.nc + f.nr) * f.nc;
+  if (!out) return cnt;
+  if (!h->factored) return fail(MFD_E_STATE, "not factorized");
+  CK(cudaSetDevice(h->device));
+  if (h->fp32) {
+    std::vector<float> tmp(cnt);
+    CK(cudaMemcpy(tmp.data(), static_cast<float*>(h->d_panel) + f.panel_off, cnt * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < cnt; ++i) out[i] = tmp[i];
+  } else {
+    CK(cudaMemcpy(out, static_cast<double*>(h->d_panel) + f.panel_off, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return cnt;
+}
+
+int mfd_set_profiling(mfd_handle* h, int32_t enable) {
+  if (!h) return fail(MFD_E_ARG, "null handle");
+  h->profiling = enable != 0;
+  std::memset(h->prof, 0, sizeof(h->prof));
+  h->pending.clear();
+  return MFD_OK;
+}
+
+int mfd_get_profile(mfd_handle* h, int32_t kind, mfd_kernel_profile* out) {
+  if (!h || !out || kind < 0 || kind >= MFD_K_COUNT) return fail(MFD_E_ARG, "bad argument");
+  *out = h->prof[kind];
+  return MFD_OK;
+}
+
+int mfd_destroy(mfd_handle* h) {
+  delete h;
+  return MFD_OK;
+}
+
+// ---- reference-named entry points: one module-global instance (hppllt_data_m.f90) ----
+static struct {
+  std::vector<int32_t> options;
+  std::vector<int32_t> order;
+  int32_t precision = MFD_PREC_FP64;
+  mfd_handle* h = nullptr;
+  double times[7] = {0, 0, 0, 0, 0, 0, 0};
+} g_ref;
+
+int hppllt_init(const int32_t* options, int32_t noptions) {
+  if (noptions != 4 || !options) {
+    std::fprintf(stderr, "incorrect size of options\n");
+    return -1;
+  }
+  g_ref.options.assign(options, options + 4);
+  return 0;
+}
+
+int hppllt_set_precision(int32_t precision) {
+  g_ref.precision = precision;
+  return 0;
+}
+
+int hppllt_set_ordering(const int32_t* order_perm, int32_t n) {
+  if (!order_perm || n <= 0) { g_ref.order.clear(); return 0; }
+  g_ref.order.assign(order_perm, order_perm + n);
+  return 0;
+}
+
+int hppllt_analyze(const int32_t* ccs_col, const int32_t* ccs_row, int32_t n) {
+  if (g_ref.options.size() != 4) return fail(MFD_E_STATE, "hppllt_init not called");
+  if (g_ref.h) { mfd_destroy(g_ref.h); g_ref.h = nullptr; }
+  mfd_options o;
+  mfd_default_options(&o);
+  o.nb = g_ref.options[0];
+  o.max_zero = g_ref.options[1];
+  o.precision = g_ref.precision;
+  const int32_t* ord = nullptr;
+  if (g_ref.options[3] == 1) {
+    if ((int32_t)g_ref.order.size() != n) return fail(MFD_E_ARG, "use_metis=1 needs an ordering (hppllt_set_ordering)");
+    ord = g_ref.order.data();
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  int rc = mfd_analyze(&g_ref.h, n, ccs_col, ccs_row, ord, &o);
+  g_ref.times[1] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return rc;
+}
+
+int hppllt_factorize(const double* a) {
+  if (!g_ref.h) return fail(MFD_E_STATE, "hppllt_analyze not called");
+  auto t0 = std::chrono::steady_clock::now();
+  int rc = mfd_factorize(g_ref.h, a);
+  g_ref.times[2] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  g_ref.times[6] = g_ref.h->factor_ms * 1e-3;
+  return rc;
+}
+
+int hppllt_solve(double* b) {
+  if (!g_ref.h) return fail(MFD_E_STATE, "hppllt_analyze not called");
+  auto t0 = std::chrono::steady_clock::now();
+  int rc = mfd_solve(g_ref.h, b, 1, g_ref.h->n_total, nullptr);
+  g_ref.times[3] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return rc;
+}
+
+int hppllt_finalize(void) {
+  g_ref.options.clear();
+  if (g_ref.h) { mfd_destroy(g_ref.h); g_ref.h = nullptr; }
+  return 0;
+}
+
+double hppllt_get_time_info(int32_t num) {
+  if (num < 1 || num > 7) return 0.0;
+  return g_ref.times[num - 1];
+}
+
+int64_t hppllt_get_cost(void) { return g_ref.h ? g_ref.h->cost : 0; }
+int64_t hppllt_get_nonzero(void) { return g_ref.h ? g_ref.h->nonzero : 0; }
+
+int64_t hppllt_get_array_size(int32_t num) {
+  // sizes of the reference's three FP64 buffers for the same partition and nb
+  // (supernode_matrix_extractor_m.f90:41-54, work_matrix_extractor_m.f90:51-74,
+  // border_matrix_extractor_m.f90:28-47)
+  if (!g_ref.h || num < 1 || num > 3) return 0;
+  const Symbolic& S = g_ref.h->sys[0];
+  const int64_t nb = g_ref.h->opt.nb;
+  auto ps = [](int64_t e) { return e < 1 ? (int64_t)0 : e * (e + 1) / 2; };
+  auto ps2 = [&](int64_t s, int64_t e) { return e < s ? (int64_t)0 : ps(e) - ps(s - 1); };
+  auto bsz = [&](int64_t idx, int64_t n) { return idx * nb > n ? n % nb : nb; };
+  int64_t total = 0;
+  for (int i = 0; i < S.num_node; ++i) {
+    int64_t nc = S.node_ptr[i + 1] - S.node_ptr[i], nr = S.lrow_ptr[i + 1] - S.lrow_ptr[i], n = nc + nr;
+    int64_t ss = nc % nb, ws = std::min(nb - ss, nr);
+    int64_t wstart = nr == 0 ? (nc - 1) / nb + 2 : nc / nb + 1;
+    int64_t nblk = (n - 1) / nb + 1;
+    if (num == 1) {
+      total += ps2(nr + 1, nc + nr) + ps(nb - 1) * (nc / nb) + ps(ss - 1);
+    } else if (num == 2) {
+      int64_t wn = nblk - wstart + 1 - 2;
+      total += nr * ws + ps(wn) * nb * nb + (nr - ws) * bsz(nblk, n);
+    } else {
+      if (ss != 0 && nr != 0) total += (n - (nc / nb) * nb) * bsz(wstart, n);
+    }
+  }
+  return total;
+}
+
+#pragma GCC visibility pop
+
+}  // extern "C"

@@ -1,0 +1,1040 @@
+// sm_100a kernels of the multifrontal numeric phase.
+//
+// Index maps (built once):      local_index, supernodal_index + assembly map,
+//                               block_local_index (reference tiling, export only)
+// Factorization, per tree level: fused one-CTA kernel for small fronts
+//                               (assembly + extend-add + partial Cholesky in
+//                               shared memory); blocked global-memory path for
+//                               large fronts (zero, assemble, extend-add per child
+//                               rank, panel POTRF+TRSM, trailing SYRK/GEMM on the
+//                               FP64 tensor pipe (DMMA) or FFMA tiles)
+// Solves:                       forward/backward per level with the same split
+// Residual / norms:             FP64 CSR SpMV for iterative refinement.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace mfd {
+
+namespace {
+
+__device__ __forceinline__ int lower_bound_dev(const int32_t* a, int n, int32_t key) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (a[mid] < key) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+template <typename T>
+__device__ __forceinline__ T dev_sqrt(T x);
+template <>
+__device__ __forceinline__ double dev_sqrt<double>(double x) { return sqrt(x); }
+template <>
+__device__ __forceinline__ float dev_sqrt<float>(float x) { return sqrtf(x); }
+
+inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+inline int clamp_grid(int64_t g, int64_t cap = 65535) { return (int)std::max<int64_t>(1, std::min<int64_t>(g, cap)); }
+
+// ============================================================================
+// index maps
+// ============================================================================
+
+// local_index (create_local_index_m.f90:10-45): for every L row r of child c,
+// its 1-based position in the parent front: the parent's own column r-first+1,
+// or nc_p + (position of r in the parent's sorted L rows).
+__global__ void k_local_index(DevFronts F, int32_t* local, int num_front) {
+  int c = blockIdx.x;
+  if (c >= num_front) return;
+  int p = F.parent[c];
+  if (p < 0) return;
+  int nrc = F.nr[c], off = F.lrow_off[c];
+  int fp = F.first[p], ncp = F.nc[p], nrp = F.nr[p];
+  const int32_t* lp = F.lrow + F.lrow_off[p];
+  for (int i = threadIdx.x; i < nrc; i += blockDim.x) {
+    int r = F.lrow[off + i];
+    int pos;
+    if (r < fp + ncp) {
+      pos = r - fp;
+    } else {
+      int q = lower_bound_dev(lp, nrp, r);
+      pos = (q < nrp && lp[q] == r) ? ncp + q : -1;      // -1: structure violation -> 0
+    }
+    local[off + i] = pos + 1;
+  }
+}
+
+// supernodal_index (create_supernodal_index_m.f90:10-40) and the assembly map:
+// one thread per permuted column; every A entry gets its front position
+// (1-based, the reference's value), the source index of its value and its
+// offset row + col*nf inside the front's panel.
+__global__ void k_assembly_map(DevFronts F, const int32_t* col_front, const int32_t* acol_ptr, const int32_t* arow,
+                               const int32_t* ccs_src, int32_t* sidx, int32_t* a_src, int32_t* a_pos, int n_total) {
+  int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n_total) return;
+  int f = col_front[col];
+  int first = F.first[f], nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
+  const int32_t* lr = F.lrow + F.lrow_off[f];
+  int jloc = col - first;
+  for (int k = acol_ptr[col]; k < acol_ptr[col + 1]; k++) {
+    int r = arow[k];
+    int pos;
+    if (r < first + nc) {
+      pos = r - first;
+    } else {
+      int q = lower_bound_dev(lr, nr, r);
+      pos = (q < nr && lr[q] == r) ? nc + q : -1;
+    }
+    sidx[k] = pos + 1;
+    a_src[k] = ccs_src[k];
+    a_pos[k] = pos < 0 ? 0 : pos + jloc * nf;
+  }
+}
+
+// block_local_index (block_local_index_creator_m.f90:13-122): a group is a
+// maximal run of a child's local index with constant (parent tile, child tile).
+__device__ __forceinline__ void bli_key(int loc, int i, int ncc, int nb, int& pt, int& ct) {
+  pt = (loc - 1) / nb + 1;            // get_matrix_num(local(i))
+  ct = (ncc + i) / nb + 1;            // get_work_num(i+1, node) = get_matrix_num(nc + i + 1)
+}
+
+__global__ void k_bli_count(DevFronts F, const int32_t* fronts, int count, int nb, int32_t* groups) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  int c = fronts[t];
+  int g = 0;
+  if (F.parent[c] >= 0) {
+    int nrc = F.nr[c], ncc = F.nc[c], pp = 0, pc = 0;
+    const int32_t* loc = F.local + F.lrow_off[c];
+    for (int i = 0; i < nrc; i++) {
+      int pt, ct;
+      bli_key(loc[i], i, ncc, nb, pt, ct);
+      if (pt != pp || ct != pc) { pp = pt; pc = ct; g++; }
+    }
+  }
+  groups[t] = g;
+}
+
+__global__ void k_bli_fill(DevFronts F, const int32_t* fronts, int count, int nb, const int32_t* group_base,
+                           const int32_t* index_base, int32_t* block_ptr, int32_t* pnum, int32_t* cnum,
+                           int32_t* offset, int32_t* rebuilt) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  int c = fronts[t];
+  int nrc = F.nr[c], ncc = F.nc[c];
+  const int32_t* loc = F.local + F.lrow_off[c];
+  int ibase = index_base[t];
+  for (int i = 0; i < nrc; i++) rebuilt[ibase + i] = (loc[i] - 1) % nb + 1;        // rebuild_val: mod2(local, nb)
+  if (F.parent[c] < 0) return;
+  int ss = ncc % nb;                                                                // border_supernode_size
+  int ws = min(nb - ss, nrc);                                                       // border_work_size
+  int g = group_base[t] - 1, pp = 0, pc = 0;
+  for (int i = 0; i < nrc; i++) {
+    int pt, ct;
+    bli_key(loc[i], i, ncc, nb, pt, ct);
+    if (pt != pp || ct != pc) {
+      pp = pt; pc = ct; g++;
+      pnum[g] = pt;
+      cnum[g] = ct;
+      block_ptr[g] = ibase + i + 1;                                                 // 1-based start of the group
+      int s = i + 1;                                                                // get_start_row_num
+      offset[g] = s <= ws ? s - 1 : (ss + s - 1) % nb;                              // get_block_offset
+    }
+  }
+}
+
+// ============================================================================
+// factorization
+// ============================================================================
+
+// Fused small front: zero, assemble A, extend-add the children in order, partial
+// Cholesky of the nc supernode columns and the Schur complement, all in shared
+// memory; writes the factor panel and the update matrix once.
+template <typename T>
+__global__ void __launch_bounds__(256) k_small_front(DevFronts F, const int32_t* list, const double* __restrict__ a,
+                                                     T* __restrict__ panel, T* __restrict__ upool, int32_t* info) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* S = reinterpret_cast<T*>(smem_raw);
+  const int f = list[blockIdx.x];
+  const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
+  const int ld = nf | 1;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+
+  for (int i = tid; i < ld * nf; i += nt) S[i] = T(0);
+  __syncthreads();
+  for (int k = F.a_beg[f] + tid; k < F.a_beg[f + 1]; k += nt) {
+    int pos = F.a_pos[k];
+    int c = pos / nf, r = pos - c * nf;
+    S[r + c * ld] = T(a[F.a_src[k]]);
+  }
+  __syncthreads();
+  for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
+    const int c = F.child[t];
+    const int nrc = F.nr[c];
+    const T* __restrict__ U = upool + F.u_off[c];
+    const int32_t* __restrict__ loc = F.local + F.lrow_off[c];
+    for (int j = warp; j < nrc; j += nw) {
+      const int lj = (loc[j] - 1) * ld;
+      const T* col = U + (size_t)j * nrc;
+      for (int i = j + lane; i < nrc; i += 32) S[(loc[i] - 1) + lj] += col[i];
+    }
+    __syncthreads();
+  }
+  for (int k = 0; k < nc; ++k) {
+    T* colk = S + k * ld;
+    if (tid == 0) {
+      T d = colk[k];
+      if (!(d > T(0))) { atomicMin(info, F.first[f] + k + 1); d = T(1); }
+      colk[k] = dev_sqrt<T>(d);
+    }
+    __syncthreads();
+    const T inv = T(1) / colk[k];
+    for (int i = k + 1 + tid; i < nf; i += nt) colk[i] *= inv;
+    __syncthreads();
+    for (int j = k + 1 + warp; j < nf; j += nw) {
+      const T ljk = colk[j];
+      T* colj = S + j * ld;
+      for (int i = j + lane; i < nf; i += 32) colj[i] -= colk[i] * ljk;
+    }
+    __syncthreads();
+  }
+  T* P = panel + F.panel_off[f];
+  for (int j = warp; j < nc; j += nw)
+    for (int i = j + lane; i < nf; i += 32) P[i + (size_t)j * nf] = S[i + j * ld];
+  T* U = upool + F.u_off[f];
+  for (int j = warp; j < nr; j += nw)
+    for (int i = j + lane; i < nr; i += 32) U[i + (size_t)j * nr] = S[(nc + i) + (nc + j) * ld];
+}
+
+template <typename T>
+__global__ void k_zero_large(DevFronts F, const int32_t* list, T* panel, T* upool) {
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
+  const int64_t np = (int64_t)nf * nc, nu = (int64_t)nr * nr;
+  T* P = panel + F.panel_off[f];
+  T* U = upool + F.u_off[f];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) P[i] = T(0);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nu; i += stride) U[i] = T(0);
+}
+
+template <typename T>
+__global__ void k_assemble_large(DevFronts F, const int32_t* list, const double* __restrict__ a, T* panel) {
+  const int f = list[blockIdx.y];
+  T* P = panel + F.panel_off[f];
+  for (int k = F.a_beg[f] + blockIdx.x * blockDim.x + threadIdx.x; k < F.a_beg[f + 1]; k += gridDim.x * blockDim.x)
+    P[F.a_pos[k]] = T(a[F.a_src[k]]);
+}
+
+// Extend-add of one child per parent (children of one rank, so no two CTAs of a
+// launch write the same parent entry): warp per child column, lanes over rows.
+template <typename T>
+__global__ void __launch_bounds__(256) k_extend_add(DevFronts F, const int32_t* list, T* panel, T* upool) {
+  const int c = list[blockIdx.y];
+  const int p = F.parent[c];
+  const int nrc = F.nr[c];
+  const int ncp = F.nc[p], nrp = F.nr[p], nfp = ncp + nrp;
+  const T* __restrict__ Uc = upool + F.u_off[c];
+  T* Pp = panel + F.panel_off[p];
+  T* Up = upool + F.u_off[p];
+  const int32_t* __restrict__ loc = F.local + F.lrow_off[c];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = blockIdx.x * nw + warp; j < nrc; j += gridDim.x * nw) {
+    const int lj = loc[j] - 1;
+    const T* src = Uc + (size_t)j * nrc;
+    if (lj < ncp) {
+      T* dst = Pp + (size_t)lj * nfp;
+      for (int i = j + lane; i < nrc; i += 32) dst[loc[i] - 1] += src[i];
+    } else {
+      T* dst = Up + (size_t)(lj - ncp) * nrp - ncp;
+      for (int i = j + lane; i < nrc; i += 32) dst[loc[i] - 1] += src[i];
+    }
+  }
+}
+
+// Panel step: Cholesky of the w x w diagonal block (redundantly in every CTA),
+// then each CTA solves kPanelRows rows of the panel below it: X <- X L11^{-T}.
+template <typename T>
+__global__ void __launch_bounds__(kPanelRows) k_panel(DevFronts F, const int32_t* list, int step, T* panel,
+                                                      T* diag_out, int32_t* info) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int B = kPanelB, LDD = kPanelB + 1;
+  T* D = reinterpret_cast<T*>(smem_raw);
+  T* invd = D + B * LDD;
+  T* X = invd + B;
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * B;
+  if (c0 >= nc) return;
+  const int w = min(B, nc - c0);
+  const int r0 = c0 + w;
+  const int rb0 = r0 + blockIdx.x * blockDim.x;
+  if (blockIdx.x > 0 && rb0 >= nf) return;
+  T* P = panel + F.panel_off[f];
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int j = e / w, i = e - j * w;
+    if (i >= j) D[i + j * LDD] = P[(c0 + i) + (size_t)(c0 + j) * nf];
+  }
+  __syncthreads();
+  for (int k = 0; k < w; ++k) {
+    if (threadIdx.x == 0) {
+      T d = D[k + k * LDD];
+      if (!(d > T(0))) {
+        if (blockIdx.x == 0) atomicMin(info, F.first[f] + c0 + k + 1);
+        d = T(1);
+      }
+      d = dev_sqrt<T>(d);
+      D[k + k * LDD] = d;
+      invd[k] = T(1) / d;
+    }
+    __syncthreads();
+    const T inv = invd[k];
+    for (int i = k + 1 + threadIdx.x; i < w; i += blockDim.x) D[i + k * LDD] *= inv;
+    __syncthreads();
+    const int rem = w - k - 1;
+    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
+      int jj = e / rem, ii = e - jj * rem;
+      if (ii >= jj) D[(k + 1 + ii) + (k + 1 + jj) * LDD] -= D[(k + 1 + ii) + k * LDD] * D[(k + 1 + jj) + k * LDD];
+    }
+    __syncthreads();
+  }
+  // Other CTAs of this launch may still be reading the unfactored block from P,
+  // so the factored block goes to scratch; the update kernel of this step
+  // copies it into the panel.
+  if (blockIdx.x == 0) {
+    T* out = diag_out + (size_t)blockIdx.y * B * B;
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+      int j = e / w, i = e - j * w;
+      if (i >= j) out[i + j * B] = D[i + j * LDD];
+    }
+  }
+  const int r = rb0 + threadIdx.x;
+  if (r < nf) {
+    T* x = X + threadIdx.x * LDD;
+    for (int k = 0; k < w; ++k) x[k] = P[r + (size_t)(c0 + k) * nf];
+    for (int k = 0; k < w; ++k) {
+      T s = x[k];
+      const T* drow = D + k;
+      for (int m = 0; m < k; ++m) s -= x[m] * drow[m * LDD];
+      x[k] = s * invd[k];
+    }
+    for (int k = 0; k < w; ++k) P[r + (size_t)(c0 + k) * nf] = x[k];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void copy_diag_block(T* P, int nf, int c0, int w, const T* src) {
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int j = e / w, i = e - j * w;
+    if (i >= j) P[(c0 + i) + (size_t)(c0 + j) * nf] = src[i + j * kPanelB];
+  }
+}
+
+__device__ __forceinline__ void tile_of(int t, int& ti, int& tj) {
+  int i = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+  while ((i + 1) * (i + 2) / 2 <= t) ++i;
+  while (i * (i + 1) / 2 > t) --i;
+  ti = i;
+  tj = t - i * (i + 1) / 2;
+}
+
+template <typename T>
+__device__ __forceinline__ T* trailing_addr(T* P, T* U, int nc, int nr, int nf, int gi, int gj) {
+  return gj < nc ? P + gi + (size_t)gj * nf : U + (gi - nc) + (size_t)(gj - nc) * nr;
+}
+
+// Trailing update on the FP64 tensor pipe: C(lower) -= P_i P_j^T for one 64x64
+// tile of the trailing matrix, P = the w <= 64 columns just factored.  4 warps,
+// each a 32x32 sub-tile of 4x4 mma.m8n8k4.f64; operands staged k-major in
+// shared memory (row stride 72 doubles: conflict-free fragment loads).
+constexpr int kLdK = 72;
+__global__ void __launch_bounds__(128) k_update_dmma(DevFronts F, const int32_t* list, int step, double* panel,
+                                                     double* upool, const double* diag_in) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* As = reinterpret_cast<double*>(smem_raw);     // [k][row], k < 64
+  double* Bs = As + kPanelB * kLdK;
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
+  const int c0 = step * kPanelB;
+  if (c0 >= nc) return;
+  const int w = min(kPanelB, nc - c0);
+  if (blockIdx.x == 0) copy_diag_block(panel + F.panel_off[f], nf, c0, w, diag_in + (size_t)blockIdx.y * kPanelB * kPanelB);
+  const int base = c0 + w;
+  const int nrem = nf - base;
+  if (nrem <= 0) return;
+  const int T = (nrem + kTile - 1) / kTile;
+  if ((int)blockIdx.x >= T * (T + 1) / 2) return;
+  int ti, tj;
+  tile_of(blockIdx.x, ti, tj);
+  const int i0 = base + ti * kTile, j0 = base + tj * kTile;
+  double* P = panel + F.panel_off[f];
+  const int wp = (w + 3) & ~3;
+  for (int e = threadIdx.x; e < kTile * wp; e += blockDim.x) {
+    int k = e / kTile, r = e - k * kTile;
+    int gi = i0 + r, gj = j0 + r;
+    bool kin = k < w;
+    As[k * kLdK + r] = (kin && gi < nf) ? P[gi + (size_t)(c0 + k) * nf] : 0.0;
+    Bs[k * kLdK + r] = (kin && gj < nf) ? P[gj + (size_t)(c0 + k) * nf] : 0.0;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int g = lane >> 2, q = lane & 3;
+  double acc[4][4][2];
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+  for (int kk = 0; kk < wp; kk += 4) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) av[mi] = As[(kk + q) * kLdK + wm * 32 + mi * 8 + g];
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(kk + q) * kLdK + wn * 32 + ni * 8 + g];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                     : "+d"(acc[mi][ni][0]), "+d"(acc[mi][ni][1])
+                     : "d"(av[mi]), "d"(bv[ni]));
+  }
+  double* U = upool + F.u_off[f];
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int gi = i0 + wm * 32 + mi * 8 + g;
+        int gj = j0 + wn * 32 + ni * 8 + 2 * q + e;
+        if (gi < nf && gj < nf && gi >= gj) *trailing_addr(P, U, nc, nr, nf, gi, gj) -= acc[mi][ni][e];
+      }
+}
+
+// Trailing update on the FMA pipes (any T): 256 threads, each 4x4 outputs of a
+// 64x64 tile (rows ty+16m, columns tx+16n).
+template <typename T>
+__global__ void __launch_bounds__(256) k_update_simt(DevFronts F, const int32_t* list, int step, T* panel, T* upool,
+                                                     const T* diag_in) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int LDK = kTile + 4;
+  T* As = reinterpret_cast<T*>(smem_raw);
+  T* Bs = As + kPanelB * LDK;
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
+  const int c0 = step * kPanelB;
+  if (c0 >= nc) return;
+  const int w = min(kPanelB, nc - c0);
+  if (blockIdx.x == 0) copy_diag_block(panel + F.panel_off[f], nf, c0, w, diag_in + (size_t)blockIdx.y * kPanelB * kPanelB);
+  const int base = c0 + w;
+  const int nrem = nf - base;
+  if (nrem <= 0) return;
+  const int Tn = (nrem + kTile - 1) / kTile;
+  if ((int)blockIdx.x >= Tn * (Tn + 1) / 2) return;
+  int ti, tj;
+  tile_of(blockIdx.x, ti, tj);
+  const int i0 = base + ti * kTile, j0 = base + tj * kTile;
+  T* P = panel + F.panel_off[f];
+  for (int e = threadIdx.x; e < kTile * w; e += blockDim.x) {
+    int k = e / kTile, r = e - k * kTile;
+    int gi = i0 + r, gj = j0 + r;
+    As[k * LDK + r] = gi < nf ? P[gi + (size_t)(c0 + k) * nf] : T(0);
+    Bs[k * LDK + r] = gj < nf ? P[gj + (size_t)(c0 + k) * nf] : T(0);
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  T acc[4][4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int n = 0; n < 4; ++n) acc[m][n] = T(0);
+  for (int k = 0; k < w; ++k) {
+    T av[4], bv[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) av[m] = As[k * LDK + ty + 16 * m];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) bv[n] = Bs[k * LDK + tx + 16 * n];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int n = 0; n < 4; ++n) acc[m][n] += av[m] * bv[n];
+  }
+  T* U = upool + F.u_off[f];
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      int gi = i0 + ty + 16 * m, gj = j0 + tx + 16 * n;
+      if (gi < nf && gj < nf && gi >= gj) *trailing_addr(P, U, nc, nr, nf, gi, gj) -= acc[m][n];
+    }
+}
+
+// ============================================================================
+// solves
+// ============================================================================
+
+// Forward solve of a small front (one CTA): v = [x(own columns); 0] plus the
+// children's update vectors through local_index, L11 y = v1, v2 -= L21 y.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwd_small(DevFronts F, const int32_t* list, const T* __restrict__ panel,
+                                                   T* X, int64_t ldx, T* V, int nrhs) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int f = list[blockIdx.x];
+  const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr, ld = nf | 1;
+  T* L = reinterpret_cast<T*>(smem_raw);
+  T* v = L + (size_t)ld * nc;
+  T* y = v + nf;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const T* P = panel + F.panel_off[f];
+  for (int j = warp; j < nc; j += nw)
+    for (int i = j + lane; i < nf; i += 32) L[i + j * ld] = P[i + (size_t)j * nf];
+  const int first = F.first[f];
+  for (int r = 0; r < nrhs; ++r) {
+    __syncthreads();
+    for (int i = tid; i < nf; i += nt) v[i] = i < nc ? X[first + i + r * ldx] : T(0);
+    __syncthreads();
+    for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
+      const int c = F.child[t];
+      const int ncc = F.nc[c], nrc = F.nr[c];
+      const T* Vc = V + F.v_off[c] * nrhs + (int64_t)r * (ncc + nrc) + ncc;
+      const int32_t* loc = F.local + F.lrow_off[c];
+      for (int i = tid; i < nrc; i += nt) v[loc[i] - 1] += Vc[i];
+      __syncthreads();
+    }
+    for (int k = 0; k < nc; ++k) {
+      const T yk = v[k] / L[k + k * ld];
+      for (int i = k + 1 + tid; i < nf; i += nt) v[i] -= L[i + k * ld] * yk;
+      if (tid == 0) y[k] = yk;
+      __syncthreads();
+    }
+    for (int i = tid; i < nc; i += nt) X[first + i + r * ldx] = y[i];
+    T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
+    for (int i = nc + tid; i < nf; i += nt) Vf[i] = v[i];
+  }
+}
+
+// Backward solve of a small front: v2 = x(L rows), t = v1 - L21^T v2,
+// L11^T y = t, x(own columns) = y.
+template <typename T>
+__global__ void __launch_bounds__(256) k_bwd_small(DevFronts F, const int32_t* list, const T* __restrict__ panel,
+                                                   T* X, int64_t ldx, int nrhs) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int f = list[blockIdx.x];
+  const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr, ld = nf | 1;
+  T* L = reinterpret_cast<T*>(smem_raw);
+  T* v = L + (size_t)ld * nc;
+  T* t = v + nf;
+  T* y = t + nc;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const T* P = panel + F.panel_off[f];
+  for (int j = warp; j < nc; j += nw)
+    for (int i = j + lane; i < nf; i += 32) L[i + j * ld] = P[i + (size_t)j * nf];
+  const int first = F.first[f];
+  const int32_t* lr = F.lrow + F.lrow_off[f];
+  for (int r = 0; r < nrhs; ++r) {
+    __syncthreads();
+    for (int i = tid; i < nf; i += nt) v[i] = i < nc ? X[first + i + r * ldx] : X[lr[i - nc] + r * ldx];
+    __syncthreads();
+    for (int k = tid; k < nc; k += nt) {
+      T s = v[k];
+      for (int i = nc; i < nf; ++i) s -= L[i + k * ld] * v[i];
+      t[k] = s;
+    }
+    __syncthreads();
+    for (int k = nc - 1; k >= 0; --k) {
+      const T yk = t[k] / L[k + k * ld];
+      for (int m = tid; m < k; m += nt) t[m] -= L[k + m * ld] * yk;
+      if (tid == 0) y[k] = yk;
+      __syncthreads();
+    }
+    for (int i = tid; i < nc; i += nt) X[first + i + r * ldx] = y[i];
+  }
+}
+
+// ---- large fronts: the solve vector of front f lives in V (nf per RHS) --------
+template <typename T>
+__global__ void k_fwd_large_gather(DevFronts F, const int32_t* list, const T* X, int64_t ldx, T* V, int nrhs) {
+  const int f = list[blockIdx.x];
+  const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
+  for (int r = 0; r < nrhs; ++r) {
+    T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
+    for (int i = threadIdx.x; i < nf; i += blockDim.x) Vf[i] = i < nc ? X[first + i + r * ldx] : T(0);
+    __syncthreads();
+    for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
+      const int c = F.child[t];
+      const int ncc = F.nc[c], nrc = F.nr[c];
+      const T* Vc = V + F.v_off[c] * nrhs + (int64_t)r * (ncc + nrc) + ncc;
+      const int32_t* loc = F.local + F.lrow_off[c];
+      for (int i = threadIdx.x; i < nrc; i += blockDim.x) Vf[loc[i] - 1] += Vc[i];
+      __syncthreads();
+    }
+  }
+}
+
+// diagonal block of panel `step`: y = L_ss^{-1} v_s (forward) in one CTA
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwd_large_diag(DevFronts F, const int32_t* list, int step,
+                                                        const T* __restrict__ panel, T* V, int nrhs) {
+  __shared__ T D[kPanelB * (kPanelB + 1)];
+  __shared__ T vs[kPanelB];
+  const int f = list[blockIdx.x];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kPanelB;
+  if (c0 >= nc) return;
+  const int w = min(kPanelB, nc - c0);
+  const T* P = panel + F.panel_off[f];
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int j = e / w, i = e - j * w;
+    if (i >= j) D[i + j * (kPanelB + 1)] = P[(c0 + i) + (size_t)(c0 + j) * nf];
+  }
+  for (int r = 0; r < nrhs; ++r) {
+    T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
+    __syncthreads();
+    for (int i = threadIdx.x; i < w; i += blockDim.x) vs[i] = Vf[c0 + i];
+    __syncthreads();
+    if (threadIdx.x < 32) {        // one warp: sequential columns, lanes over rows
+      for (int k = 0; k < w; ++k) {
+        T yk = vs[k] / D[k + k * (kPanelB + 1)];
+        __syncwarp();
+        for (int i = k + 1 + threadIdx.x; i < w; i += 32) vs[i] -= D[i + k * (kPanelB + 1)] * yk;
+        if (threadIdx.x == 0) vs[k] = yk;
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < w; i += blockDim.x) Vf[c0 + i] = vs[i];
+  }
+}
+
+// rows below the diagonal block: v_i -= sum_k L(i, c0+k) y_k
+template <typename T>
+__global__ void __launch_bounds__(kSolveRows) k_fwd_large_gemv(DevFronts F, const int32_t* list, int step,
+                                                               const T* __restrict__ panel, T* V, int nrhs) {
+  __shared__ T ys[kPanelB];
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kPanelB;
+  if (c0 >= nc) return;
+  const int w = min(kPanelB, nc - c0);
+  const int i = c0 + w + blockIdx.x * blockDim.x + threadIdx.x;
+  if (c0 + w + blockIdx.x * blockDim.x >= nf) return;
+  const T* P = panel + F.panel_off[f];
+  for (int r = 0; r < nrhs; ++r) {
+    T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
+    __syncthreads();
+    if (threadIdx.x < w) ys[threadIdx.x] = Vf[c0 + threadIdx.x];
+    __syncthreads();
+    if (i < nf) {
+      T s = T(0);
+      for (int k = 0; k < w; ++k) s += P[i + (size_t)(c0 + k) * nf] * ys[k];
+      Vf[i] -= s;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_fwd_large_finish(DevFronts F, const int32_t* list, T* X, int64_t ldx, const T* V, int nrhs) {
+  const int f = list[blockIdx.x];
+  const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
+  for (int r = 0; r < nrhs; ++r) {
+    const T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) X[first + i + r * ldx] = Vf[i];
+  }
+}
+
+template <typename T>
+__global__ void k_bwd_large_gather(DevFronts F, const int32_t* list, const T* X, int64_t ldx, T* V, int nrhs) {
+  const int f = list[blockIdx.x];
+  const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
+  const int32_t* lr = F.lrow + F.lrow_off[f];
+  for (int r = 0; r < nrhs; ++r) {
+    T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
+    for (int i = threadIdx.x; i < nf; i += blockDim.x) Vf[i] = i < nc ? X[first + i + r * ldx] : X[lr[i - nc] + r * ldx];
+  }
+}
+
+// partial sums of L(rows of this CTA, panel)^T v(rows): lanes over rows, warp reductions
+template <typename T>
+__global__ void __launch_bounds__(kSolveRows) k_bwd_large_gemvt(DevFronts F, const int32_t* list, int step,
+                                                                const T* __restrict__ panel, const T* V, T* scratch,
+                                                                int nrhs) {
+  __shared__ T part[kSolveRows / 32][kPanelB];
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kPanelB;
+  if (c0 >= nc) return;
+  const int w = min(kPanelB, nc - c0);
+  const int rstart = c0 + w + blockIdx.x * blockDim.x;
+  const int nchunks = (nf - c0 - w + kSolveRows - 1) / kSolveRows;
+  if (rstart >= nf) return;
+  const int i = rstart + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const T* P = panel + F.panel_off[f];
+  for (int r = 0; r < nrhs; ++r) {
+    const T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
+    const T vi = i < nf ? Vf[i] : T(0);
+    for (int k = 0; k < w; ++k) {
+      T s = i < nf ? P[i + (size_t)(c0 + k) * nf] * vi : T(0);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) part[warp][k] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < w) {
+      T s = T(0);
+      for (int q = 0; q < kSolveRows / 32; ++q) s += part[q][threadIdx.x];
+      scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + blockIdx.x) * kPanelB + threadIdx.x] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// diagonal block (backward): t = v_s - sum of partial sums; L_ss^T y = t
+template <typename T>
+__global__ void __launch_bounds__(256) k_bwd_large_diag(DevFronts F, const int32_t* list, int step,
+                                                        const T* __restrict__ panel, T* V, const T* scratch,
+                                                        int nrhs) {
+  __shared__ T D[kPanelB * (kPanelB + 1)];
+  __shared__ T ts[kPanelB];
+  const int f = list[blockIdx.x];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kPanelB;
+  if (c0 >= nc) return;
+  const int w = min(kPanelB, nc - c0);
+  const int nchunks = (nf - c0 - w + kSolveRows - 1) / kSolveRows;
+  const T* P = panel + F.panel_off[f];
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    int j = e / w, i = e - j * w;
+    if (i >= j) D[i + j * (kPanelB + 1)] = P[(c0 + i) + (size_t)(c0 + j) * nf];
+  }
+  for (int r = 0; r < nrhs; ++r) {
+    T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
+    __syncthreads();
+    for (int k = threadIdx.x; k < w; k += blockDim.x) {
+      T s = Vf[c0 + k];
+      for (int q = 0; q < nchunks; ++q) s -= scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + q) * kPanelB + k];
+      ts[k] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      for (int k = w - 1; k >= 0; --k) {
+        T yk = ts[k] / D[k + k * (kPanelB + 1)];
+        __syncwarp();
+        for (int m = threadIdx.x; m < k; m += 32) ts[m] -= D[k + m * (kPanelB + 1)] * yk;
+        if (threadIdx.x == 0) ts[k] = yk;
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < w; k += blockDim.x) Vf[c0 + k] = ts[k];
+  }
+}
+
+// ============================================================================
+// vectors
+// ============================================================================
+template <typename T>
+__global__ void k_permute_in(const double* b, int64_t ldb, const int32_t* perm, T* X, int64_t ldx, int64_t n, int nrhs) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t src = perm[i];
+    for (int r = 0; r < nrhs; ++r) X[i + r * ldx] = T(b[src + r * ldb]);
+  }
+}
+template <typename T>
+__global__ void k_permute_out(const T* X, int64_t ldx, const int32_t* perm, double* b, int64_t ldb, int64_t n, int nrhs) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t dst = perm[i];
+    for (int r = 0; r < nrhs; ++r) b[dst + r * ldb] = double(X[i + r * ldx]);
+  }
+}
+__global__ void k_gather_values(const double* a, const int32_t* src, double* out, int64_t count) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = a[src[i]];
+}
+__global__ void k_residual(const int64_t* rowptr, const int32_t* col, const double* val, const double* x,
+                           const double* b, double* r, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e) s += val[e] * x[col[e]];
+    r[i] = b[i] - s;
+  }
+}
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), __double_as_longlong(v));
+}
+__global__ void k_norms(const double* r, const double* x, const double* b, int64_t n, double* out) {
+  double mr = 0, mx = 0, mb = 0, sr = 0, sx = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double a = fabs(r[i]), c = fabs(x[i]), d = fabs(b[i]);
+    mr = fmax(mr, a); mx = fmax(mx, c); mb = fmax(mb, d);
+    sr += r[i] * r[i]; sx += x[i] * x[i];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+    sr += __shfl_xor_sync(0xffffffffu, sr, o);
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_nonneg(out + 0, mr);
+    atomic_max_nonneg(out + 1, mx);
+    atomic_max_nonneg(out + 2, mb);
+    atomicAdd(out + 3, sr);
+    atomicAdd(out + 4, sx);
+  }
+}
+__global__ void k_row_abs_max(const int64_t* rowptr, const double* val, int64_t n, double* out) {
+  double m = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0;
+    for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e) s += fabs(val[e]);
+    m = fmax(m, s);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, m);
+}
+template <typename T>
+__global__ void k_to_t(const double* in, T* out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = T(in[i]);
+}
+template <typename T>
+__global__ void k_axpy_from_t(const T* d, double* x, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += double(d[i]);
+}
+__global__ void k_fill_int(int32_t* p, int32_t v, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+inline int grid_1d(int64_t n, int threads = 256) { return clamp_grid(ceil_div(n, threads), 148 * 16); }
+
+template <typename T>
+size_t small_front_smem(int nf_max) { return (size_t)(nf_max | 1) * nf_max * sizeof(T); }
+template <typename T>
+size_t fwd_small_smem(int nf_max) { return ((size_t)(nf_max | 1) * nf_max + 3 * nf_max) * sizeof(T); }
+
+// Dynamic shared memory above 48 KB is opted into once per kernel at handle
+// creation (prepare_kernels), never inside a stream capture.
+constexpr int kMaxDynSmem = 227 * 1024;
+template <typename KernelT>
+cudaError_t opt_in(KernelT k) {
+  return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+}
+template <typename KernelT>
+void set_smem(KernelT, size_t) {}
+
+}  // namespace
+
+// ============================================================================
+// launch wrappers
+// ============================================================================
+cudaError_t prepare_kernels() {
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t r) { if (r != cudaSuccess && e == cudaSuccess) e = r; };
+  chk(opt_in(k_small_front<double>)); chk(opt_in(k_small_front<float>));
+  chk(opt_in(k_panel<double>)); chk(opt_in(k_panel<float>));
+  chk(opt_in(k_update_dmma));
+  chk(opt_in(k_update_simt<double>)); chk(opt_in(k_update_simt<float>));
+  chk(opt_in(k_fwd_small<double>)); chk(opt_in(k_fwd_small<float>));
+  chk(opt_in(k_bwd_small<double>)); chk(opt_in(k_bwd_small<float>));
+  return e;
+}
+
+void launch_local_index(const DevFronts& F, int32_t* local, int num_front, cudaStream_t st) {
+  if (num_front > 0) k_local_index<<<num_front, 128, 0, st>>>(F, local, num_front);
+}
+void launch_assembly_map(const DevFronts& F, const int32_t* col_front, const int32_t* acol_ptr, const int32_t* arow,
+                         const int32_t* ccs_src, int32_t* sidx, int32_t* a_src, int32_t* a_pos, int n_total,
+                         cudaStream_t st) {
+  if (n_total > 0)
+    k_assembly_map<<<ceil_div(n_total, 256), 256, 0, st>>>(F, col_front, acol_ptr, arow, ccs_src, sidx, a_src, a_pos,
+                                                           n_total);
+}
+void launch_bli_count(const DevFronts& F, const int32_t* fronts, int count, int nb, int32_t* groups, cudaStream_t st) {
+  if (count > 0) k_bli_count<<<ceil_div(count, 128), 128, 0, st>>>(F, fronts, count, nb, groups);
+}
+void launch_bli_fill(const DevFronts& F, const int32_t* fronts, int count, int nb, const int32_t* group_base,
+                     const int32_t* index_base, int32_t* block_ptr, int32_t* pnum, int32_t* cnum, int32_t* offset,
+                     int32_t* rebuilt, cudaStream_t st) {
+  if (count > 0)
+    k_bli_fill<<<ceil_div(count, 128), 128, 0, st>>>(F, fronts, count, nb, group_base, index_base, block_ptr, pnum,
+                                                     cnum, offset, rebuilt);
+}
+
+template <typename T>
+void launch_small_fronts(const DevFronts& F, const int32_t* list, int count, int nf_max, const double* a, T* panel,
+                         T* upool, int32_t* info, cudaStream_t st) {
+  if (count <= 0) return;
+  size_t sm = small_front_smem<T>(nf_max);
+  set_smem(k_small_front<T>, sm);
+  k_small_front<T><<<count, 256, sm, st>>>(F, list, a, panel, upool, info);
+}
+template <typename T>
+void launch_zero_large(const DevFronts& F, const int32_t* list, int count, int64_t max_elems, T* panel, T* upool,
+                       cudaStream_t st) {
+  if (count <= 0) return;
+  dim3 grid(clamp_grid(ceil_div(max_elems, 256 * 4), 1024), count);
+  k_zero_large<T><<<grid, 256, 0, st>>>(F, list, panel, upool);
+}
+template <typename T>
+void launch_assemble_large(const DevFronts& F, const int32_t* list, int count, int max_entries, const double* a,
+                           T* panel, cudaStream_t st) {
+  if (count <= 0) return;
+  dim3 grid(clamp_grid(ceil_div(max_entries, 256), 256), count);
+  k_assemble_large<T><<<grid, 256, 0, st>>>(F, list, a, panel);
+}
+template <typename T>
+void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int max_nr, T* panel, T* upool,
+                       cudaStream_t st) {
+  if (count <= 0) return;
+  dim3 grid(clamp_grid(ceil_div(max_nr, 8), 1024), count);
+  k_extend_add<T><<<grid, 256, 0, st>>>(F, list, panel, upool);
+}
+template <typename T>
+void launch_panel(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
+                  T* diag_scratch, int32_t* info, cudaStream_t st) {
+  if (count <= 0) return;
+  size_t sm = ((size_t)kPanelB * (kPanelB + 1) + kPanelB + (size_t)kPanelRows * (kPanelB + 1)) * sizeof(T);
+  set_smem(k_panel<T>, sm);
+  dim3 grid(std::max(1, row_blocks), count);
+  k_panel<T><<<grid, kPanelRows, sm, st>>>(F, list, step, panel, diag_scratch, info);
+}
+template <typename T>
+void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles, T* panel, T* upool,
+                   const T* diag_scratch, int kind, cudaStream_t st) {
+  if (count <= 0) return;
+  dim3 grid(std::max(1, tiles), count);
+  if constexpr (sizeof(T) == 8) {
+    if (kind == 0) {
+      size_t sm = 2 * (size_t)kPanelB * kLdK * sizeof(double);
+      set_smem(k_update_dmma, sm);
+      k_update_dmma<<<grid, 128, sm, st>>>(F, list, step, reinterpret_cast<double*>(panel),
+                                           reinterpret_cast<double*>(upool),
+                                           reinterpret_cast<const double*>(diag_scratch));
+      return;
+    }
+  }
+  size_t sm = 2 * (size_t)kPanelB * (kTile + 4) * sizeof(T);
+  set_smem(k_update_simt<T>, sm);
+  k_update_simt<T><<<grid, 256, sm, st>>>(F, list, step, panel, upool, diag_scratch);
+}
+
+template <typename T>
+void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
+                      int64_t ldx, T* V, int nrhs, cudaStream_t st) {
+  if (count <= 0) return;
+  size_t sm = fwd_small_smem<T>(nf_max);
+  set_smem(k_fwd_small<T>, sm);
+  k_fwd_small<T><<<count, 256, sm, st>>>(F, list, panel, X, ldx, V, nrhs);
+}
+template <typename T>
+void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
+                      int64_t ldx, int nrhs, cudaStream_t st) {
+  if (count <= 0) return;
+  size_t sm = fwd_small_smem<T>(nf_max);
+  set_smem(k_bwd_small<T>, sm);
+  k_bwd_small<T><<<count, 256, sm, st>>>(F, list, panel, X, ldx, nrhs);
+}
+template <typename T>
+void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
+                      T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st, int64_t* launches) {
+  if (count <= 0) return;
+  k_fwd_large_gather<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
+  int steps = ceil_div(max_nc, kPanelB);
+  int chunks = std::max(1, ceil_div(max_nf, kSolveRows));
+  for (int s = 0; s < steps; ++s) {
+    k_fwd_large_diag<T><<<count, 256, 0, st>>>(F, list, s, panel, V, nrhs);
+    k_fwd_large_gemv<T><<<dim3(chunks, count), kSolveRows, 0, st>>>(F, list, s, panel, V, nrhs);
+  }
+  k_fwd_large_finish<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
+  if (launches) *launches += 2 + 2 * steps;
+}
+template <typename T>
+void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
+                      T* X, int64_t ldx, T* V, T* scratch, int nrhs, cudaStream_t st, int64_t* launches) {
+  if (count <= 0) return;
+  k_bwd_large_gather<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
+  int steps = ceil_div(max_nc, kPanelB);
+  int chunks = std::max(1, ceil_div(max_nf, kSolveRows));
+  for (int s = steps - 1; s >= 0; --s) {
+    k_bwd_large_gemvt<T><<<dim3(chunks, count), kSolveRows, 0, st>>>(F, list, s, panel, V, scratch, nrhs);
+    k_bwd_large_diag<T><<<count, 256, 0, st>>>(F, list, s, panel, V, scratch, nrhs);
+  }
+  k_fwd_large_finish<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
+  if (launches) *launches += 2 + 2 * steps;
+}
+
+template <typename T>
+void launch_permute_in(const double* b, int64_t ldb, const int32_t* perm, T* X, int64_t ldx, int64_t n, int nrhs,
+                       cudaStream_t st) {
+  k_permute_in<T><<<grid_1d(n), 256, 0, st>>>(b, ldb, perm, X, ldx, n, nrhs);
+}
+template <typename T>
+void launch_permute_out(const T* X, int64_t ldx, const int32_t* perm, double* b, int64_t ldb, int64_t n, int nrhs,
+                        cudaStream_t st) {
+  k_permute_out<T><<<grid_1d(n), 256, 0, st>>>(X, ldx, perm, b, ldb, n, nrhs);
+}
+void launch_gather_values(const double* a, const int32_t* src, double* out, int64_t count, cudaStream_t st) {
+  if (count > 0) k_gather_values<<<grid_1d(count), 256, 0, st>>>(a, src, out, count);
+}
+void launch_residual(const int64_t* rowptr, const int32_t* col, const double* val, const double* x, const double* b,
+                     double* r, int64_t n, cudaStream_t st) {
+  k_residual<<<grid_1d(n), 256, 0, st>>>(rowptr, col, val, x, b, r, n);
+}
+void launch_norms(const double* r, const double* x, const double* b, int64_t n, double* out, cudaStream_t st) {
+  cudaMemsetAsync(out, 0, 5 * sizeof(double), st);
+  k_norms<<<grid_1d(n), 256, 0, st>>>(r, x, b, n, out);
+}
+void launch_row_abs_max(const int64_t* rowptr, const double* val, int64_t n, double* out, cudaStream_t st) {
+  cudaMemsetAsync(out, 0, sizeof(double), st);
+  k_row_abs_max<<<grid_1d(n), 256, 0, st>>>(rowptr, val, n, out);
+}
+template <typename T>
+void launch_to_t(const double* in, T* out, int64_t n, cudaStream_t st) {
+  k_to_t<T><<<grid_1d(n), 256, 0, st>>>(in, out, n);
+}
+template <typename T>
+void launch_axpy_from_t(const T* d, double* x, int64_t n, cudaStream_t st) {
+  k_axpy_from_t<T><<<grid_1d(n), 256, 0, st>>>(d, x, n);
+}
+void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
+  if (n > 0) k_fill_int<<<grid_1d(n), 256, 0, st>>>(p, v, n);
+}
+
+#define MFD_INSTANTIATE(T)                                                                                          \
+  template void launch_small_fronts<T>(const DevFronts&, const int32_t*, int, int, const double*, T*, T*, int32_t*, \
+                                       cudaStream_t);                                                              \
+  template void launch_zero_large<T>(const DevFronts&, const int32_t*, int, int64_t, T*, T*, cudaStream_t);         \
+  template void launch_assemble_large<T>(const DevFronts&, const int32_t*, int, int, const double*, T*,             \
+                                         cudaStream_t);                                                            \
+  template void launch_extend_add<T>(const DevFronts&, const int32_t*, int, int, T*, T*, cudaStream_t);             \
+  template void launch_panel<T>(const DevFronts&, const int32_t*, int, int, int, T*, T*, int32_t*, cudaStream_t);   \
+  template void launch_update<T>(const DevFronts&, const int32_t*, int, int, int, T*, T*, const T*, int,            \
+                                 cudaStream_t);                                                                    \
+  template void launch_fwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, T*, int,     \
+                                    cudaStream_t);                                                                 \
+  template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, int,         \
+                                    cudaStream_t);                                                                 \
+  template void launch_fwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, T*, int64_t, T*,     \
+                                    int, cudaStream_t, int64_t*);                                                  \
+  template void launch_bwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, T*, int64_t, T*, T*, \
+                                    int, cudaStream_t, int64_t*);                                                  \
+  template void launch_permute_in<T>(const double*, int64_t, const int32_t*, T*, int64_t, int64_t, int,            \
+                                     cudaStream_t);                                                                \
+  template void launch_permute_out<T>(const T*, int64_t, const int32_t*, double*, int64_t, int64_t, int,           \
+                                      cudaStream_t);                                                               \
+  template void launch_to_t<T>(const double*, T*, int64_t, cudaStream_t);                                          \
+  template void launch_axpy_from_t<T>(const T*, double*, int64_t, cudaStream_t);
+
+MFD_INSTANTIATE(double)
+MFD_INSTANTIATE(float)
+
+}  // namespace mfd

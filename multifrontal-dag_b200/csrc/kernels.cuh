@@ -1,0 +1,88 @@
+// Launch wrappers of the sm_100a kernels (kernels.cu).  Every wrapper enqueues
+// on `st` and returns nothing; errors surface through cudaGetLastError /
+// stream synchronisation in the caller.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "plan.hpp"
+
+namespace mfd {
+
+constexpr int kPanelB = 64;          // column panel of the blocked large-front factorization
+constexpr int kPanelRows = 128;      // rows per CTA in the panel TRSM
+constexpr int kTile = 64;            // trailing-update output tile
+constexpr int kSolveRows = 256;      // rows per CTA in the large-front solve GEMV kernels
+
+// Opt every shared-memory-heavy kernel into the large dynamic shared memory
+// carve-out; called once per process before any launch or capture.
+cudaError_t prepare_kernels();
+
+// ---- index maps (built once per handle) ------------------------------------
+void launch_local_index(const DevFronts& F, int32_t* local, int num_front, cudaStream_t st);
+void launch_assembly_map(const DevFronts& F, const int32_t* col_front, const int32_t* acol_ptr, const int32_t* arow,
+                         const int32_t* ccs_src, int32_t* sidx, int32_t* a_src, int32_t* a_pos, int n_total,
+                         cudaStream_t st);
+void launch_bli_count(const DevFronts& F, const int32_t* fronts, int count, int nb, int32_t* groups, cudaStream_t st);
+void launch_bli_fill(const DevFronts& F, const int32_t* fronts, int count, int nb, const int32_t* group_base,
+                     const int32_t* index_base, int32_t* block_ptr, int32_t* pnum, int32_t* cnum, int32_t* offset,
+                     int32_t* rebuilt, cudaStream_t st);
+
+// ---- factorization -----------------------------------------------------------
+template <typename T>
+void launch_small_fronts(const DevFronts& F, const int32_t* list, int count, int nf_max, const double* a, T* panel,
+                         T* upool, int32_t* info, cudaStream_t st);
+template <typename T>
+void launch_zero_large(const DevFronts& F, const int32_t* list, int count, int64_t max_elems, T* panel, T* upool,
+                       cudaStream_t st);
+template <typename T>
+void launch_assemble_large(const DevFronts& F, const int32_t* list, int count, int max_entries, const double* a,
+                           T* panel, cudaStream_t st);
+template <typename T>
+void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int max_nr, T* panel, T* upool,
+                       cudaStream_t st);
+// The factored diagonal block of each front goes to diag_scratch (count x 64 x 64)
+// and the update launch of the same step copies it into the panel.
+template <typename T>
+void launch_panel(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
+                  T* diag_scratch, int32_t* info, cudaStream_t st);
+template <typename T>
+void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles, T* panel, T* upool,
+                   const T* diag_scratch, int kind, cudaStream_t st);
+
+// ---- solves --------------------------------------------------------------------
+template <typename T>
+void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
+                      int64_t ldx, T* V, int nrhs, cudaStream_t st);
+template <typename T>
+void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
+                      int64_t ldx, int nrhs, cudaStream_t st);
+template <typename T>
+void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
+                      T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st, int64_t* launches);
+template <typename T>
+void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
+                      T* X, int64_t ldx, T* V, T* scratch, int nrhs, cudaStream_t st, int64_t* launches);
+
+// ---- vectors, residuals ---------------------------------------------------------
+template <typename T>
+void launch_permute_in(const double* b, int64_t ldb, const int32_t* perm_global, T* X, int64_t ldx, int64_t n,
+                       int nrhs, cudaStream_t st);
+template <typename T>
+void launch_permute_out(const T* X, int64_t ldx, const int32_t* perm_global, double* b, int64_t ldb, int64_t n,
+                        int nrhs, cudaStream_t st);
+void launch_gather_values(const double* a, const int32_t* src, double* out, int64_t count, cudaStream_t st);
+// r = b - A x (permuted full CSR, FP64), with |A| |x| row sums for the backward error
+void launch_residual(const int64_t* rowptr, const int32_t* col, const double* val, const double* x, const double* b,
+                     double* r, int64_t n, cudaStream_t st);
+// out[0]=max|r|, out[1]=max|x|, out[2]=max|b|, out[3]=sum r^2, out[4]=sum x^2 (per column 0 of nrhs)
+void launch_norms(const double* r, const double* x, const double* b, int64_t n, double* out, cudaStream_t st);
+void launch_row_abs_max(const int64_t* rowptr, const double* val, int64_t n, double* out, cudaStream_t st);
+template <typename T>
+void launch_to_t(const double* in, T* out, int64_t n, cudaStream_t st);
+template <typename T>
+void launch_axpy_from_t(const T* d, double* x, int64_t n, cudaStream_t st);
+void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st);
+
+}  // namespace mfd

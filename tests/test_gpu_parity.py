@@ -1,0 +1,269 @@
+"""GPU parity tests: the sm_100a path through the C ABI against the CPU oracle.
+
+Integer index data (local_index, supernodal_index, block_local_index) must be
+bit-exact; FP64 factors and solutions within the tolerances written below;
+FP32 + FP64 iterative refinement to backward error <= 1e-12.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from golden import reference_vectors as R
+from helpers import lower_panel, oracle_front_panel, toy_symbolic
+from mfdag import hppllt as H
+from mfdag import problems as P
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+FP64_X_TOL = 1e-10        # ||x - x_oracle||_inf / ||x_oracle||_inf (both FP64, different summation order)
+FP64_BWD_TOL = 1e-12      # normwise backward error
+FACTOR_TOL = 1e-12        # relative entrywise difference of factor panels
+
+
+def oracle_for(p, nb=10, max_zero=10):
+    o = O.Oracle.analyze(p.n, p.col, p.row, nb=nb, max_zero=max_zero, order_perm=p.order)
+    assert o.factorize(p.val) == 0
+    return o
+
+
+def gpu_for(p, max_zero=10, **opts):
+    s = H.Solver.analyze(p.n, p.col, p.row, p.order, max_zero=max_zero, **opts)
+    assert s.factorize(p.val) == 0
+    return s
+
+
+# ---------------------------------------------------------------------------
+# the reference's own numeric fixture
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("nb", [2, 3])
+def test_toy_factor_matches_reference_vectors(nb):
+    sym = toy_symbolic()
+    s = H.Solver.from_symbolic(sym, nb=nb)
+    assert s.factorize(np.array(R.TOY_VALUES, np.float64)) == 0
+    o = O.Oracle.from_internal(R.TOY_NODE_SIZE, [len(x) for x in sym["lrows"]], sym["lrow"], R.TOY_PARENT, 13,
+                               sym["aptr"], sym["arow"], nb)
+    assert o.factorize(np.array(R.TOY_VALUES, np.float64)) == 0
+    for node in (1, 2, 3):
+        nc, nr = R.TOY_NODE_SIZE[node - 1], R.TOY_WORK_SIZE[node - 1]
+        got = lower_panel(s.front_panel(node), nc + nr, nc)
+        ref = oracle_front_panel(o, node, nc, nr, nb)
+        assert np.allclose(got, ref, rtol=0, atol=1e-12), node
+        assert np.array_equal(np.round(got), ref)          # the fixture's factor is integer-valued
+    # index data built on the device
+    assert list(s.index(H.LOCAL_INDEX)) == R.TOY_LOCAL_VAL
+    assert list(s.index(H.SUPERNODAL_INDEX)) == R.TOY_SIDX_VAL
+
+
+@pytest.mark.parametrize("nb", [2, 3])
+def test_toy_solve(nb):
+    sym = toy_symbolic()
+    s = H.Solver.from_symbolic(sym, nb=nb)
+    assert s.factorize(np.array(R.TOY_VALUES, np.float64)) == 0
+    # A x = b with x = 1: b = L L^T 1 from the oracle's sweeps run backwards is not
+    # available, so build A from the values and check the residual directly
+    n = 13
+    A = np.zeros((n, n))
+    for j in range(n):
+        for k in range(sym["aptr"][j] - 1, sym["aptr"][j + 1] - 1):
+            r = sym["arow"][k] - 1
+            A[r, j] = A[j, r] = R.TOY_VALUES[k]
+    x_true = np.arange(1, n + 1, dtype=np.float64)
+    b = A @ x_true
+    x = b.copy()
+    rep, rc = s.solve(x)
+    assert rc == 0
+    assert np.allclose(x, x_true, rtol=1e-12, atol=1e-12)
+
+
+# ---------------------------------------------------------------------------
+# index maps: bit-exact with the oracle (reference semantics)
+# ---------------------------------------------------------------------------
+def index_cases():
+    yield "lap2d_30", P.laplace2d(30), 10, 10
+    yield "lap2d_30_nb4", P.laplace2d(30), 4, 10
+    yield "lap3d_12", P.laplace3d(12), 10, 10
+    yield "lap3d_12_mz1000", P.laplace3d(12), 7, 1000
+    yield "diff3d_10", P.diffusion3d(10), 10, 10
+
+
+@pytest.mark.parametrize("name,p,nb,mz", list(index_cases()), ids=[c[0] for c in index_cases()])
+def test_index_maps_bit_exact(name, p, nb, mz):
+    s = H.Solver.analyze(p.n, p.col, p.row, p.order, max_zero=mz, nb=nb)
+    o = O.Oracle.analyze(p.n, p.col, p.row, nb=nb, max_zero=mz, order_perm=p.order)
+    assert np.array_equal(s.index(H.LOCAL_INDEX), o.get(O.LOCAL))
+    assert np.array_equal(s.index(H.SUPERNODAL_INDEX), o.get(O.SIDX))
+    assert np.array_equal(s.index(H.BLI_NODE_PTR), o.get(O.BLI_NODE_PTR))
+    assert np.array_equal(s.index(H.BLI_BLOCK_PTR), o.get(O.BLI_BLOCK_PTR))
+    assert np.array_equal(s.index(H.BLI_PARENT), o.get(O.BLI_PARENT))
+    assert np.array_equal(s.index(H.BLI_CHILD), o.get(O.BLI_CHILD))
+    assert np.array_equal(s.index(H.BLI_VAL), o.get(O.BLI_VAL))
+    assert np.array_equal(s.index(H.BLI_OFFSET), o.get(O.BLI_OFFSET))
+
+
+# ---------------------------------------------------------------------------
+# FP64 factor + solve
+# ---------------------------------------------------------------------------
+def check_solution(p, s, o, tol=FP64_X_TOL):
+    x = p.rhs.copy()
+    rep, rc = s.solve(x)
+    assert rc == 0
+    xo = o.solve(p.rhs)
+    rel = np.abs(x - xo).max() / np.abs(xo).max()
+    assert rel <= tol, rel
+    bwd = P.backward_error(p.n, p.col, p.row, p.val, x, p.rhs)
+    assert bwd <= FP64_BWD_TOL, bwd
+    assert rep.backward_error <= FP64_BWD_TOL
+    assert abs(rep.backward_error - bwd) <= 1e-3 * max(bwd, 1e-300) + 1e-18
+    return x
+
+
+def test_laplace2d_100_fp64():                 # 2D 5-point, 100x100 (n = 10,000), x* from seed 0
+    p = P.laplace2d(100)
+    check_solution(p, gpu_for(p), oracle_for(p))
+
+
+@pytest.mark.parametrize("small_max", [0, 48])
+def test_laplace3d_fp64_large_path(small_max):
+    """16^3 Laplacian; small_front_max=48 forces the blocked large-front kernels
+    (zero/assemble/extend-add/panel/update) onto many fronts."""
+    p = P.laplace3d(16)
+    s = gpu_for(p, max_zero=10, small_front_max=small_max)
+    o = oracle_for(p)
+    check_solution(p, s, o)
+    # factor panels of the largest fronts against the oracle's tiles
+    sym = o.symbolic()
+    nc = np.diff(sym["node_ptr"]); nr = np.diff(sym["lptr"])
+    for node in np.argsort(-(nc + nr))[:3] + 1:
+        a, b = int(nc[node - 1]), int(nr[node - 1])
+        got = lower_panel(s.front_panel(int(node)), a + b, a)
+        ref = oracle_front_panel(o, int(node), a, b, 10)
+        assert np.abs(got - ref).max() <= FACTOR_TOL * np.abs(ref).max()
+
+
+def test_update_kernel_variants_agree():
+    """DMMA and FFMA trailing updates give the same factor to rounding."""
+    p = P.laplace3d(14)
+    s0 = gpu_for(p, small_front_max=40)
+    opts = H.default_options(small_front_max=40)
+    s1 = H.Solver.analyze(p.n, p.col, p.row, p.order, max_zero=10, small_front_max=40,
+                          reserved=(1, 0, 0, 0, 0, 0, 0))
+    assert s1.factorize(p.val) == 0
+    x0, x1 = p.rhs.copy(), p.rhs.copy()
+    s0.solve(x0)
+    s1.solve(x1)
+    assert np.abs(x0 - x1).max() <= 1e-12 * np.abs(x0).max()
+    del opts
+
+
+def test_multiple_rhs():
+    p = P.laplace2d(40)
+    s = gpu_for(p)
+    o = oracle_for(p)
+    rng = np.random.default_rng(7)
+    B = np.asfortranarray(rng.uniform(-1, 1, (p.n, 3)))
+    X = B.copy(order="F")
+    rep, rc = s.solve(X)
+    assert rc == 0
+    for r in range(3):
+        xo = o.solve(B[:, r])
+        assert np.abs(X[:, r] - xo).max() <= FP64_X_TOL * np.abs(xo).max()
+
+
+def test_deterministic_replay():
+    p = P.laplace3d(12)
+    s = gpu_for(p, small_front_max=40)
+    x1 = p.rhs.copy(); s.solve(x1)
+    assert s.factorize(p.val) == 0
+    x2 = p.rhs.copy(); s.solve(x2)
+    assert np.array_equal(x1, x2)
+
+
+def test_without_graphs_matches():
+    p = P.laplace2d(30)
+    s0 = gpu_for(p)
+    s1 = gpu_for(p, use_graph=0)
+    x0, x1 = p.rhs.copy(), p.rhs.copy()
+    s0.solve(x0); s1.solve(x1)
+    assert np.array_equal(x0, x1)
+
+
+def test_not_positive_definite_reports_pivot():
+    p = P.laplace2d(12)
+    val = p.val.copy()
+    diag_pos = p.col[:-1] - 1                  # diagonal entries come first in each column
+    val[diag_pos[5]] = -4.0
+    s = H.Solver.analyze(p.n, p.col, p.row, p.order)
+    info = s.factorize(val)
+    assert info > 0
+    with pytest.raises(H.MfdError) as e:
+        s.solve(p.rhs.copy())
+    assert e.value.code == -6
+
+
+# ---------------------------------------------------------------------------
+# FP32 factor + FP64 iterative refinement
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("mk", [lambda: P.laplace3d(16), lambda: P.diffusion3d(12)], ids=["lap3d", "diff3d"])
+def test_fp32_ir_reaches_1e12(mk):
+    p = mk()
+    s = gpu_for(p, precision=H.MFD_PREC_FP32_IR, small_front_max=64)
+    x = p.rhs.copy()
+    rep, rc = s.solve(x)
+    assert rc == 0 and rep.converged == 1
+    assert rep.iterations >= 1
+    bwd = P.backward_error(p.n, p.col, p.row, p.val, x, p.rhs)
+    assert bwd <= 1e-12, bwd
+    xo = oracle_for(p).solve(p.rhs)
+    assert np.abs(x - xo).max() <= 1e-8 * np.abs(xo).max()
+
+
+# ---------------------------------------------------------------------------
+# batch of independent systems (uneven sizes)
+# ---------------------------------------------------------------------------
+def test_batch_uneven():
+    probs = P.laplace2d_batch(count=12, seed=3, lo=8, hi=40)
+    s = H.Solver.analyze_batch([(q.n, q.col, q.row, q.order) for q in probs])
+    a = np.concatenate([q.val for q in probs])
+    assert s.factorize(a) == 0
+    b = np.concatenate([q.rhs for q in probs])
+    x = b.copy()
+    rep, rc = s.solve(x)
+    assert rc == 0
+    off = 0
+    for i, q in enumerate(probs):
+        o = O.Oracle.analyze(q.n, q.col, q.row, nb=10, max_zero=10, order_perm=q.order)
+        assert o.factorize(q.val) == 0
+        xo = o.solve(q.rhs)
+        xi = x[off:off + q.n]
+        assert np.abs(xi - xo).max() <= FP64_X_TOL * np.abs(xo).max(), i
+        # per-system device index data equals the oracle's
+        assert np.array_equal(s.index(H.LOCAL_INDEX, i), o.get(O.LOCAL))
+        off += q.n
+
+
+# ---------------------------------------------------------------------------
+# the reference-named API on the reference's own end-to-end fixtures
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", ["bcsstk01.mtx", "poisson_9_9.mtx"])
+def test_hppllt_api_fixture(name):
+    from test_oracle_e2e import coo_to_ccs, sym_matvec
+    m = json.load(open(os.path.join(HERE, "golden", "mtx_fixtures.json")))[name]
+    n = m["n"]
+    ptr, row, val = coo_to_ccs(n, m["row"], m["col"], m["val"])
+    H.hppllt_init(R.HPPLLT_TEST_OPTIONS)
+    H.hppllt_analyze(ptr, row, n)
+    assert H.hppllt_factorize(val) == 0
+    b = np.full(n, 10.0)
+    H.hppllt_solve(b)
+    r = 10.0 - sym_matvec(n, ptr, row, val, b)
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= R.HPPLLT_TEST_TOL
+    assert H.hppllt_get_cost() > 0 and H.hppllt_get_nonzero() > 0
+    o = O.Oracle.analyze(n, ptr, row, nb=10, max_zero=10)
+    assert H.hppllt_get_cost() == o.cost()
+    for k in (1, 2, 3):
+        assert H.hppllt_get_array_size(k) == o.array_size(k)
+    H.hppllt_finalize()

@@ -169,12 +169,13 @@ int64_t mfd_get_front_panel(mfd_handle *h, int32_t system, int32_t node, double 
 #define MFD_K_ZERO 1          /* large-front zero fill                         */
 #define MFD_K_ASSEMBLE 2      /* large-front assembly of A                     */
 #define MFD_K_EXTEND_ADD 3    /* large-front extend-add                        */
-#define MFD_K_PANEL 4         /* panel POTRF + TRSM                            */
+#define MFD_K_PANEL 4         /* diagonal-block POTRF + inverse                */
 #define MFD_K_UPDATE 5        /* trailing SYRK/GEMM update                     */
 #define MFD_K_SOLVE_SMALL 6   /* one-CTA forward/backward solves               */
 #define MFD_K_SOLVE_LARGE 7   /* blocked forward/backward solves               */
 #define MFD_K_OTHER 8         /* permutations, residuals, norms                */
-#define MFD_K_COUNT 9
+#define MFD_K_TRSM 9          /* panel TRSM (rows below the diagonal block)    */
+#define MFD_K_COUNT 10
 typedef struct {
   int64_t launches;
   double ms;

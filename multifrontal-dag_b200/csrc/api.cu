@@ -280,7 +280,7 @@ int build_plan(mfd_handle* h) {
     fr.v_off = h->v_elems;
     h->v_elems += nf;
     fr.s_off = h->s_elems;
-    if (nf > sfm) h->s_elems += (int64_t)((nf + kSolveRows - 1) / kSolveRows) * kPanelB;
+    if (nf > sfm) h->s_elems += (int64_t)((nf + kSolveRows - 1) / kSolveRows) * kSolveB;
   }
   // update pool: static first-fit plan over level lifetimes
   {
@@ -344,7 +344,7 @@ int build_plan(mfd_handle* h) {
       const HostFront& fr = h->fronts[g];
       int nf = fr.nc + fr.nr;
       max_entries = std::max(max_entries, h->h_a_beg[g + 1] - h->h_a_beg[g]);
-      max_elems = std::max(max_elems, std::max<int64_t>((int64_t)nf * fr.nc, (int64_t)fr.nr * fr.nr));
+      max_elems = std::max<int64_t>(max_elems, nf);
       max_nc = std::max(max_nc, fr.nc);
       L.large_max_nf = std::max(L.large_max_nf, nf);
     }
@@ -370,24 +370,27 @@ int build_plan(mfd_handle* h) {
       L.ext_add.push_back(ll);
     }
     // panel steps: prefix of the nc-sorted list
-    int steps = (max_nc + kPanelB - 1) / kPanelB;
+    int steps = (max_nc + kFactB - 1) / kFactB;
     for (int s = 0; s < steps; ++s) {
       LaunchList ll;
       ll.off = L.large.off;
-      int cntf = 0, rows = 1, tiles = 1;
+      int cntf = 0, rows = 0, tiles128 = 0, tiles64 = 0;
       for (int32_t g : large) {
         const HostFront& fr = h->fronts[g];
-        if (fr.nc <= s * kPanelB) break;
+        if (fr.nc <= s * kFactB) break;
         ++cntf;
-        int w = std::min(kPanelB, fr.nc - s * kPanelB);
-        int nrem = fr.nc + fr.nr - s * kPanelB - w;
-        rows = std::max(rows, (nrem + kPanelRows - 1) / kPanelRows);
-        int T = (nrem + kTile - 1) / kTile;
-        tiles = std::max(tiles, T * (T + 1) / 2);
+        int w = std::min(kFactB, fr.nc - s * kFactB);
+        int nrem = fr.nc + fr.nr - s * kFactB - w;
+        rows = std::max(rows, (nrem + kTrRowsH - 1) / kTrRowsH);
+        int T = (nrem + kUpdTile - 1) / kUpdTile;
+        tiles128 = std::max(tiles128, T * (T + 1) / 2);
+        int T6 = (nrem + kUpdTileSimt - 1) / kUpdTileSimt;
+        tiles64 = std::max(tiles64, T6 * (T6 + 1) / 2);
       }
       ll.count = cntf;
       ll.param = rows;
-      ll.param2 = tiles;
+      ll.param2 = tiles128;
+      ll.param3 = tiles64;
       L.steps.push_back(ll);
     }
   }
@@ -581,7 +584,7 @@ int upload_plan(mfd_handle* h) {
   size_t esz = h->fp32 ? sizeof(float) : sizeof(double);
   CK(cudaMalloc(&h->d_panel, std::max<int64_t>(h->panel_elems, 1) * esz));
   CK(cudaMalloc(&h->d_upool, std::max<int64_t>(h->upool_elems, 1) * esz));
-  CK(cudaMalloc(&h->d_diag, (size_t)std::max(1, h->max_large_count) * kPanelB * kPanelB * esz));
+  CK(cudaMalloc(&h->d_diag, (size_t)std::max(1, h->max_large_count) * kFactB * kFactB * esz));
   CK(h->d_a.alloc(h->nnz_total));
   CK(h->d_norms.alloc(8));
   return MFD_OK;
@@ -685,7 +688,7 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
     if (prof)
       for (int i = 0; i < L.large.count; ++i) {
         const HostFront& f = h->fronts[hl[L.large.off + i]];
-        zb += w * ((double)(f.nc + f.nr) * f.nc + (double)f.nr * f.nr);
+        zb += w * ((double)(f.nc + f.nr) * f.nc - (double)f.nc * (f.nc - 1) / 2 + (double)f.nr * (f.nr + 1) / 2);
         ab += 12.0 * (h->h_a_beg[hl[L.large.off + i] + 1] - h->h_a_beg[hl[L.large.off + i]]);
       }
     record(h, st, MFD_K_ZERO, 0, zb,
@@ -707,23 +710,27 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
     }
     for (size_t s = 0; s < L.steps.size(); ++s) {
       const LaunchList& p = L.steps[s];
-      double pf = 0, pb = 0, uf = 0, ub = 0;
+      double pf = 0, pb = 0, tf = 0, tb = 0, uf = 0, ub = 0;
       if (prof)
         for (int i = 0; i < p.count; ++i) {
           const HostFront& f = h->fronts[hl[p.off + i]];
-          double c0 = (double)s * kPanelB, wd = std::min<double>(kPanelB, f.nc - c0);
+          double c0 = (double)s * kFactB, wd = std::min<double>(kFactB, f.nc - c0);
           double nrem = f.nc + f.nr - c0 - wd;
-          pf += wd * wd * wd / 3 + nrem * wd * wd;
-          pb += w * (wd * wd / 2 + nrem * wd) * 2;
+          pf += wd * wd * wd / 3 + wd * wd * wd / 3;            // POTRF + triangular inverse
+          pb += w * wd * wd * 2;
+          tf += 2.0 * nrem * wd * wd;                          // X = A Li^T
+          tb += w * (2.0 * nrem * wd + wd * wd);
           uf += 2.0 * wd * nrem * (nrem + 1) / 2;
           ub += w * (2.0 * nrem * (nrem + 1) / 2 + 2.0 * nrem * wd);
         }
       record(h, st, MFD_K_PANEL, pf, pb,
-             [&] { launch_panel<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, h->d_info.p, st); });
+             [&] { launch_potrf<T>(F, lists + p.off, p.count, (int)s, panel, diag, h->d_info.p, st); });
+      record(h, st, MFD_K_TRSM, tf, tb,
+             [&] { launch_trsm<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, kind, st); });
       record(h, st, MFD_K_UPDATE, uf, ub, [&] {
-        launch_update<T>(F, lists + p.off, p.count, (int)s, p.param2, panel, upool, diag, kind, st);
+        launch_update<T>(F, lists + p.off, p.count, (int)s, p.param2, p.param3, panel, upool, kind, st);
       });
-      n += 2;
+      n += 3;
     }
   }
   // values of the permuted full matrix for residuals

@@ -132,7 +132,7 @@ __global__ void k_bli_fill(DevFronts F, const int32_t* fronts, int count, int nb
   if (F.parent[c] < 0) return;
   int ss = ncc % nb;                                                                // border_supernode_size
   int ws = min(nb - ss, nrc);                                                       // border_work_size
-  int g = group_base[t] - 1, pp = 0, pc = 0;
+  int g = group_base[t] - 2, pp = 0, pc = 0;                                       // 0-based, before the first group
   for (int i = 0; i < nrc; i++) {
     int pt, ct;
     bli_key(loc[i], i, ncc, nb, pt, ct);
@@ -211,16 +211,25 @@ __global__ void __launch_bounds__(256) k_small_front(DevFronts F, const int32_t*
     for (int i = j + lane; i < nr; i += 32) U[i + (size_t)j * nr] = S[(nc + i) + (nc + j) * ld];
 }
 
+// Zero the lower triangles of a large front's panel (nf x nc) and update
+// matrix (nr x nr): one warp per column, grid-stride over columns.
 template <typename T>
 __global__ void k_zero_large(DevFronts F, const int32_t* list, T* panel, T* upool) {
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
-  const int64_t np = (int64_t)nf * nc, nu = (int64_t)nr * nr;
   T* P = panel + F.panel_off[f];
   T* U = upool + F.u_off[f];
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) P[i] = T(0);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nu; i += stride) U[i] = T(0);
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int j = blockIdx.x * nw + (threadIdx.x >> 5); j < nc + nr; j += gridDim.x * nw) {
+    if (j < nc) {
+      T* col = P + (size_t)j * nf;
+      for (int i = j + lane; i < nf; i += 32) col[i] = T(0);
+    } else {
+      const int jj = j - nc;
+      T* col = U + (size_t)jj * nr;
+      for (int i = jj + lane; i < nr; i += 32) col[i] = T(0);
+    }
+  }
 }
 
 template <typename T>
@@ -257,82 +266,210 @@ __global__ void __launch_bounds__(256) k_extend_add(DevFronts F, const int32_t* 
   }
 }
 
-// Panel step: Cholesky of the w x w diagonal block (redundantly in every CTA),
-// then each CTA solves kPanelRows rows of the panel below it: X <- X L11^{-T}.
+// ---- blocked large-front factorization: per panel step s (columns c0 = s*128) ----
+//   k_potrf : one CTA per front: Cholesky of the w x w diagonal block in shared
+//             memory, written back as L11, then inverted in place (lower
+//             triangular) and stored as L11^{-1} in per-front scratch
+//   k_trsm  : the rows below, X <- A L11^{-T} = A (L11^{-1})^T, a GEMM with K = w
+//   k_update: trailing C(lower) -= P P^T with P the solved panel rows
+
 template <typename T>
-__global__ void __launch_bounds__(kPanelRows) k_panel(DevFronts F, const int32_t* list, int step, T* panel,
-                                                      T* diag_out, int32_t* info) {
+__global__ void __launch_bounds__(256) k_potrf(DevFronts F, const int32_t* list, int step, T* panel, T* linv,
+                                               int32_t* info) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int B = kPanelB, LDD = kPanelB + 1;
+  constexpr int B = kFactB, LDD = kFactB + 1;
   T* D = reinterpret_cast<T*>(smem_raw);
-  T* invd = D + B * LDD;
-  T* X = invd + B;
-  const int f = list[blockIdx.y];
+  T* piv = D + B * LDD;          // pivots of the unscaled elimination, then 1/L_jj of the inverse
+  const int f = list[blockIdx.x];
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int c0 = step * B;
   if (c0 >= nc) return;
   const int w = min(B, nc - c0);
-  const int r0 = c0 + w;
-  const int rb0 = r0 + blockIdx.x * blockDim.x;
-  if (blockIdx.x > 0 && rb0 >= nf) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   T* P = panel + F.panel_off[f];
-  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-    int j = e / w, i = e - j * w;
-    if (i >= j) D[i + j * LDD] = P[(c0 + i) + (size_t)(c0 + j) * nf];
+  for (int j = warp; j < w; j += nw)
+    for (int i = j + lane; i < w; i += 32) D[i + j * LDD] = P[(c0 + i) + (size_t)(c0 + j) * nf];
+  __syncthreads();
+  // Cholesky with deferred column scaling: step k subtracts c_k c_k^T / d_k from
+  // the trailing triangle using the unscaled column c_k, so one barrier per
+  // column suffices; L(:,k) = c_k / sqrt(d_k) is applied afterwards.
+  for (int k = 0; k < w; ++k) {
+    T d = D[k + k * LDD];
+    if (!(d > T(0))) {
+      if (tid == 0) atomicMin(info, F.first[f] + c0 + k + 1);
+      d = T(1);
+    }
+    if (tid == 0) piv[k] = d;
+    const T inv_d = T(1) / d;
+    for (int j = k + 1 + warp; j < w; j += nw) {
+      const T ljk = D[j + k * LDD] * inv_d;
+      for (int i = j + lane; i < w; i += 32) D[i + j * LDD] -= D[i + k * LDD] * ljk;
+    }
+    __syncthreads();
+  }
+  for (int j = warp; j < w; j += nw) {
+    const T sd = dev_sqrt<T>(piv[j]);
+    const T inv = T(1) / sd;
+    for (int i = j + lane; i < w; i += 32) {
+      T v = i == j ? sd : D[i + j * LDD] * inv;
+      D[i + j * LDD] = v;
+      P[(c0 + i) + (size_t)(c0 + j) * nf] = v;
+    }
   }
   __syncthreads();
-  for (int k = 0; k < w; ++k) {
-    if (threadIdx.x == 0) {
-      T d = D[k + k * LDD];
-      if (!(d > T(0))) {
-        if (blockIdx.x == 0) atomicMin(info, F.first[f] + c0 + k + 1);
-        d = T(1);
-      }
-      d = dev_sqrt<T>(d);
-      D[k + k * LDD] = d;
-      invd[k] = T(1) / d;
+  // in-place inverse of L11 by forward substitution on the identity, one row
+  // per step; the scaling of pivot row j by 1/L_jj is deferred to step j+1
+  // (no other thread reads row j after step j), so one barrier per row.
+  for (int j = 0; j < w; ++j) {
+    const T r = T(1) / D[j + j * LDD];
+    if (tid == 0) piv[j] = r;
+    for (int i = j + 1 + warp; i < w; i += nw) {
+      const T lik = D[i + j * LDD] * r;
+      __syncwarp();
+      for (int jp = lane; jp < j; jp += 32) D[i + jp * LDD] -= lik * D[j + jp * LDD];
+      if (lane == 0) D[i + j * LDD] = -lik;
     }
-    __syncthreads();
-    const T inv = invd[k];
-    for (int i = k + 1 + threadIdx.x; i < w; i += blockDim.x) D[i + k * LDD] *= inv;
-    __syncthreads();
-    const int rem = w - k - 1;
-    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
-      int jj = e / rem, ii = e - jj * rem;
-      if (ii >= jj) D[(k + 1 + ii) + (k + 1 + jj) * LDD] -= D[(k + 1 + ii) + k * LDD] * D[(k + 1 + jj) + k * LDD];
+    if (j >= 1) {
+      const T rp = piv[j - 1];
+      for (int jp = tid; jp < j - 1; jp += blockDim.x) D[(j - 1) + jp * LDD] *= rp;
+      if (tid == 0) D[(j - 1) + (j - 1) * LDD] = rp;
     }
     __syncthreads();
   }
-  // Other CTAs of this launch may still be reading the unfactored block from P,
-  // so the factored block goes to scratch; the update kernel of this step
-  // copies it into the panel.
-  if (blockIdx.x == 0) {
-    T* out = diag_out + (size_t)blockIdx.y * B * B;
-    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-      int j = e / w, i = e - j * w;
-      if (i >= j) out[i + j * B] = D[i + j * LDD];
-    }
+  {
+    const T rp = piv[w - 1];
+    for (int jp = tid; jp < w - 1; jp += blockDim.x) D[(w - 1) + jp * LDD] *= rp;
+    if (tid == 0) D[(w - 1) + (w - 1) * LDD] = rp;
   }
-  const int r = rb0 + threadIdx.x;
-  if (r < nf) {
-    T* x = X + threadIdx.x * LDD;
-    for (int k = 0; k < w; ++k) x[k] = P[r + (size_t)(c0 + k) * nf];
-    for (int k = 0; k < w; ++k) {
-      T s = x[k];
-      const T* drow = D + k;
-      for (int m = 0; m < k; ++m) s -= x[m] * drow[m * LDD];
-      x[k] = s * invd[k];
-    }
-    for (int k = 0; k < w; ++k) P[r + (size_t)(c0 + k) * nf] = x[k];
-  }
+  __syncthreads();
+  T* Li = linv + (size_t)blockIdx.x * B * B;          // column-major, ld = B, zero outside the lower w x w
+  for (int j = warp; j < B; j += nw)
+    for (int i = lane; i < B; i += 32) Li[i + j * B] = (i >= j && i < w && j < w) ? D[i + j * LDD] : T(0);
 }
 
-template <typename T>
-__device__ __forceinline__ void copy_diag_block(T* P, int nf, int c0, int w, const T* src) {
-  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-    int j = e / w, i = e - j * w;
-    if (i >= j) P[(c0 + i) + (size_t)(c0 + j) * nf] = src[i + j * kPanelB];
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc, bool valid) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+  int sz = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// TRSM on the FP64 tensor pipe: 64 rows x w columns of the panel per CTA,
+// X = A Li^T with Li = L11^{-1}; 8 warps as 2 (rows) x 4 (columns) of 32x32.
+constexpr int kTrRows = 64, kTrLdA = 72, kTrLdB = 136;
+__global__ void __launch_bounds__(256, 1) k_trsm_dmma(DevFronts F, const int32_t* list, int step, double* panel,
+                                                      const double* linv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* As = reinterpret_cast<double*>(smem_raw);      // [k][row], k < 128
+  double* Bs = As + kFactB * kTrLdA;                      // [k][n]
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kFactB;
+  if (c0 >= nc) return;
+  const int w = min(kFactB, nc - c0);
+  const int r0 = c0 + w + blockIdx.x * kTrRows;
+  if (r0 >= nf) return;
+  double* P = panel + F.panel_off[f];
+  const double* Li = linv + (size_t)blockIdx.y * kFactB * kFactB;
+  const int wp = (w + 3) & ~3;
+  for (int e = threadIdx.x; e < kTrRows * wp; e += blockDim.x) {
+    int k = e / kTrRows, r = e - k * kTrRows;
+    As[k * kTrLdA + r] = (k < w && r0 + r < nf) ? P[(r0 + r) + (size_t)(c0 + k) * nf] : 0.0;
   }
+  for (int e = threadIdx.x; e < kFactB * wp; e += blockDim.x) {
+    int k = e / kFactB, n = e - k * kFactB;
+    Bs[k * kTrLdB + n] = Li[n + k * kFactB];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp >> 2, wn = warp & 3;
+  const int g = lane >> 2, q = lane & 3;
+  double acc[4][4][2];
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+  for (int kk = 0; kk < wp; kk += 4) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) av[mi] = As[(kk + q) * kTrLdA + wm * 32 + mi * 8 + g];
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(kk + q) * kTrLdB + wn * 32 + ni * 8 + g];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], av[mi], bv[ni]);
+  }
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int gi = r0 + wm * 32 + mi * 8 + g;
+        int n = wn * 32 + ni * 8 + 2 * q + e;
+        if (gi < nf && n < w) P[gi + (size_t)(c0 + n) * nf] = acc[mi][ni][e];
+      }
+}
+
+// TRSM on the FMA pipes (any T): 64 rows x w columns, thread = 4 rows x 8 columns.
+template <typename T>
+__global__ void __launch_bounds__(256) k_trsm_simt(DevFronts F, const int32_t* list, int step, T* panel,
+                                                   const T* linv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int LDA = kTrRows + 4, LDB = kFactB + 4;
+  T* As = reinterpret_cast<T*>(smem_raw);
+  T* Bs = As + kFactB * LDA;
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kFactB;
+  if (c0 >= nc) return;
+  const int w = min(kFactB, nc - c0);
+  const int r0 = c0 + w + blockIdx.x * kTrRows;
+  if (r0 >= nf) return;
+  T* P = panel + F.panel_off[f];
+  const T* Li = linv + (size_t)blockIdx.y * kFactB * kFactB;
+  for (int e = threadIdx.x; e < kTrRows * w; e += blockDim.x) {
+    int k = e / kTrRows, r = e - k * kTrRows;
+    As[k * LDA + r] = (r0 + r < nf) ? P[(r0 + r) + (size_t)(c0 + k) * nf] : T(0);
+  }
+  for (int e = threadIdx.x; e < kFactB * w; e += blockDim.x) {
+    int k = e / kFactB, n = e - k * kFactB;
+    Bs[k * LDB + n] = Li[n + k * kFactB];
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  T acc[4][8];
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int n = 0; n < 8; ++n) acc[m][n] = T(0);
+  for (int k = 0; k < w; ++k) {
+    T av[4], bv[8];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) av[m] = As[k * LDA + ty + 16 * m];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) bv[n] = Bs[k * LDB + tx + 16 * n];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int n = 0; n < 8; ++n) acc[m][n] += av[m] * bv[n];
+  }
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      int gi = r0 + ty + 16 * m, c = tx + 16 * n;
+      if (gi < nf && c < w) P[gi + (size_t)(c0 + c) * nf] = acc[m][n];
+    }
 }
 
 __device__ __forceinline__ void tile_of(int t, int& ti, int& tj) {
@@ -348,122 +485,139 @@ __device__ __forceinline__ T* trailing_addr(T* P, T* U, int nc, int nr, int nf, 
   return gj < nc ? P + gi + (size_t)gj * nf : U + (gi - nc) + (size_t)(gj - nc) * nr;
 }
 
-// Trailing update on the FP64 tensor pipe: C(lower) -= P_i P_j^T for one 64x64
-// tile of the trailing matrix, P = the w <= 64 columns just factored.  4 warps,
-// each a 32x32 sub-tile of 4x4 mma.m8n8k4.f64; operands staged k-major in
-// shared memory (row stride 72 doubles: conflict-free fragment loads).
-constexpr int kLdK = 72;
-__global__ void __launch_bounds__(128) k_update_dmma(DevFronts F, const int32_t* list, int step, double* panel,
-                                                     double* upool, const double* diag_in) {
+// Trailing update on the FP64 tensor pipe: one 128x128 tile of the trailing
+// lower triangle per CTA, C -= P_i P_j^T over K = w <= 128 in chunks of 32,
+// double-buffered with cp.async; 8 warps as 2 (rows) x 4 (columns) of 64x32
+// (8x4 mma.m8n8k4.f64 each).  Shared-memory operands are k-major with a row
+// stride of 136 doubles, which makes the fragment loads conflict-free.
+constexpr int kUT = 128, kUK = 32, kULD = 136;
+__global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32_t* list, int step, double* panel,
+                                                        double* upool) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* As = reinterpret_cast<double*>(smem_raw);     // [k][row], k < 64
-  double* Bs = As + kPanelB * kLdK;
+  double* sm = reinterpret_cast<double*>(smem_raw);     // [stage][operand][k][row]
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
-  const int c0 = step * kPanelB;
+  const int c0 = step * kFactB;
   if (c0 >= nc) return;
-  const int w = min(kPanelB, nc - c0);
-  if (blockIdx.x == 0) copy_diag_block(panel + F.panel_off[f], nf, c0, w, diag_in + (size_t)blockIdx.y * kPanelB * kPanelB);
+  const int w = min(kFactB, nc - c0);
   const int base = c0 + w;
   const int nrem = nf - base;
   if (nrem <= 0) return;
-  const int T = (nrem + kTile - 1) / kTile;
+  const int T = (nrem + kUT - 1) / kUT;
   if ((int)blockIdx.x >= T * (T + 1) / 2) return;
   int ti, tj;
   tile_of(blockIdx.x, ti, tj);
-  const int i0 = base + ti * kTile, j0 = base + tj * kTile;
+  const int i0 = base + ti * kUT, j0 = base + tj * kUT;
   double* P = panel + F.panel_off[f];
-  const int wp = (w + 3) & ~3;
-  for (int e = threadIdx.x; e < kTile * wp; e += blockDim.x) {
-    int k = e / kTile, r = e - k * kTile;
-    int gi = i0 + r, gj = j0 + r;
-    bool kin = k < w;
-    As[k * kLdK + r] = (kin && gi < nf) ? P[gi + (size_t)(c0 + k) * nf] : 0.0;
-    Bs[k * kLdK + r] = (kin && gj < nf) ? P[gj + (size_t)(c0 + k) * nf] : 0.0;
-  }
-  __syncthreads();
+  const int nchunks = (w + kUK - 1) / kUK;
+  auto load = [&](int stage, int kc) {
+    double* dst = sm + stage * (2 * kUK * kULD);
+    for (int e = threadIdx.x; e < 2 * kUK * kUT; e += blockDim.x) {
+      int op = e / (kUK * kUT), rem = e - op * (kUK * kUT);
+      int k = rem / kUT, r = rem - k * kUT;
+      int row = (op == 0 ? i0 : j0) + r, col = kc * kUK + k;
+      bool valid = row < nf && col < w;
+      const double* src = valid ? P + row + (size_t)(c0 + col) * nf : P;
+      cp_async8(dst + op * (kUK * kULD) + k * kULD + r, src, valid);
+    }
+    cp_async_commit();
+  };
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wm = warp >> 1, wn = warp & 1;
+  const int wm = warp >> 2, wn = warp & 3;
   const int g = lane >> 2, q = lane & 3;
-  double acc[4][4][2];
+  double acc[8][4][2];
 #pragma unroll
-  for (int mi = 0; mi < 4; ++mi)
+  for (int mi = 0; mi < 8; ++mi)
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
-  for (int kk = 0; kk < wp; kk += 4) {
-    double av[4], bv[4];
+  load(0, 0);
+  for (int kc = 0; kc < nchunks; ++kc) {
+    if (kc + 1 < nchunks) {
+      load((kc + 1) & 1, kc + 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double* As = sm + (kc & 1) * (2 * kUK * kULD);
+    const double* Bs = As + kUK * kULD;
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi) av[mi] = As[(kk + q) * kLdK + wm * 32 + mi * 8 + g];
+    for (int kk = 0; kk < kUK; kk += 4) {
+      double av[8], bv[4];
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(kk + q) * kLdK + wn * 32 + ni * 8 + g];
+      for (int mi = 0; mi < 8; ++mi) av[mi] = As[(kk + q) * kULD + wm * 64 + mi * 8 + g];
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi)
+      for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(kk + q) * kULD + wn * 32 + ni * 8 + g];
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni)
-        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                     : "+d"(acc[mi][ni][0]), "+d"(acc[mi][ni][1])
-                     : "d"(av[mi]), "d"(bv[ni]));
+      for (int mi = 0; mi < 8; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], av[mi], bv[ni]);
+    }
+    __syncthreads();
   }
   double* U = upool + F.u_off[f];
 #pragma unroll
-  for (int mi = 0; mi < 4; ++mi)
+  for (int mi = 0; mi < 8; ++mi)
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
-        int gi = i0 + wm * 32 + mi * 8 + g;
+        int gi = i0 + wm * 64 + mi * 8 + g;
         int gj = j0 + wn * 32 + ni * 8 + 2 * q + e;
         if (gi < nf && gj < nf && gi >= gj) *trailing_addr(P, U, nc, nr, nf, gi, gj) -= acc[mi][ni][e];
       }
 }
 
-// Trailing update on the FMA pipes (any T): 256 threads, each 4x4 outputs of a
-// 64x64 tile (rows ty+16m, columns tx+16n).
+// Trailing update on the FMA pipes (any T): 64x64 tiles, K in chunks of 64,
+// 256 threads each 4x4 outputs (rows ty+16m, columns tx+16n).
+constexpr int kSimtTile = 64, kSimtK = 64;
 template <typename T>
-__global__ void __launch_bounds__(256) k_update_simt(DevFronts F, const int32_t* list, int step, T* panel, T* upool,
-                                                     const T* diag_in) {
+__global__ void __launch_bounds__(256) k_update_simt(DevFronts F, const int32_t* list, int step, T* panel, T* upool) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int LDK = kTile + 4;
+  constexpr int LDK = kSimtTile + 4;
   T* As = reinterpret_cast<T*>(smem_raw);
-  T* Bs = As + kPanelB * LDK;
+  T* Bs = As + kSimtK * LDK;
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
-  const int c0 = step * kPanelB;
+  const int c0 = step * kFactB;
   if (c0 >= nc) return;
-  const int w = min(kPanelB, nc - c0);
-  if (blockIdx.x == 0) copy_diag_block(panel + F.panel_off[f], nf, c0, w, diag_in + (size_t)blockIdx.y * kPanelB * kPanelB);
+  const int w = min(kFactB, nc - c0);
   const int base = c0 + w;
   const int nrem = nf - base;
   if (nrem <= 0) return;
-  const int Tn = (nrem + kTile - 1) / kTile;
+  const int Tn = (nrem + kSimtTile - 1) / kSimtTile;
   if ((int)blockIdx.x >= Tn * (Tn + 1) / 2) return;
   int ti, tj;
   tile_of(blockIdx.x, ti, tj);
-  const int i0 = base + ti * kTile, j0 = base + tj * kTile;
+  const int i0 = base + ti * kSimtTile, j0 = base + tj * kSimtTile;
   T* P = panel + F.panel_off[f];
-  for (int e = threadIdx.x; e < kTile * w; e += blockDim.x) {
-    int k = e / kTile, r = e - k * kTile;
-    int gi = i0 + r, gj = j0 + r;
-    As[k * LDK + r] = gi < nf ? P[gi + (size_t)(c0 + k) * nf] : T(0);
-    Bs[k * LDK + r] = gj < nf ? P[gj + (size_t)(c0 + k) * nf] : T(0);
-  }
-  __syncthreads();
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   T acc[4][4];
 #pragma unroll
   for (int m = 0; m < 4; ++m)
 #pragma unroll
     for (int n = 0; n < 4; ++n) acc[m][n] = T(0);
-  for (int k = 0; k < w; ++k) {
-    T av[4], bv[4];
+  for (int k0 = 0; k0 < w; k0 += kSimtK) {
+    const int kw = min(kSimtK, w - k0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < kSimtTile * kw; e += blockDim.x) {
+      int k = e / kSimtTile, r = e - k * kSimtTile;
+      int gi = i0 + r, gj = j0 + r;
+      As[k * LDK + r] = gi < nf ? P[gi + (size_t)(c0 + k0 + k) * nf] : T(0);
+      Bs[k * LDK + r] = gj < nf ? P[gj + (size_t)(c0 + k0 + k) * nf] : T(0);
+    }
+    __syncthreads();
+    for (int k = 0; k < kw; ++k) {
+      T av[4], bv[4];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) av[m] = As[k * LDK + ty + 16 * m];
+      for (int m = 0; m < 4; ++m) av[m] = As[k * LDK + ty + 16 * m];
 #pragma unroll
-    for (int n = 0; n < 4; ++n) bv[n] = Bs[k * LDK + tx + 16 * n];
+      for (int n = 0; n < 4; ++n) bv[n] = Bs[k * LDK + tx + 16 * n];
 #pragma unroll
-    for (int m = 0; m < 4; ++m)
+      for (int m = 0; m < 4; ++m)
 #pragma unroll
-      for (int n = 0; n < 4; ++n) acc[m][n] += av[m] * bv[n];
+        for (int n = 0; n < 4; ++n) acc[m][n] += av[m] * bv[n];
+    }
   }
   T* U = upool + F.u_off[f];
 #pragma unroll
@@ -581,17 +735,17 @@ __global__ void k_fwd_large_gather(DevFronts F, const int32_t* list, const T* X,
 template <typename T>
 __global__ void __launch_bounds__(256) k_fwd_large_diag(DevFronts F, const int32_t* list, int step,
                                                         const T* __restrict__ panel, T* V, int nrhs) {
-  __shared__ T D[kPanelB * (kPanelB + 1)];
-  __shared__ T vs[kPanelB];
+  __shared__ T D[kSolveB * (kSolveB + 1)];
+  __shared__ T vs[kSolveB];
   const int f = list[blockIdx.x];
   const int nc = F.nc[f], nf = nc + F.nr[f];
-  const int c0 = step * kPanelB;
+  const int c0 = step * kSolveB;
   if (c0 >= nc) return;
-  const int w = min(kPanelB, nc - c0);
+  const int w = min(kSolveB, nc - c0);
   const T* P = panel + F.panel_off[f];
   for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
     int j = e / w, i = e - j * w;
-    if (i >= j) D[i + j * (kPanelB + 1)] = P[(c0 + i) + (size_t)(c0 + j) * nf];
+    if (i >= j) D[i + j * (kSolveB + 1)] = P[(c0 + i) + (size_t)(c0 + j) * nf];
   }
   for (int r = 0; r < nrhs; ++r) {
     T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
@@ -600,9 +754,9 @@ __global__ void __launch_bounds__(256) k_fwd_large_diag(DevFronts F, const int32
     __syncthreads();
     if (threadIdx.x < 32) {        // one warp: sequential columns, lanes over rows
       for (int k = 0; k < w; ++k) {
-        T yk = vs[k] / D[k + k * (kPanelB + 1)];
+        T yk = vs[k] / D[k + k * (kSolveB + 1)];
         __syncwarp();
-        for (int i = k + 1 + threadIdx.x; i < w; i += 32) vs[i] -= D[i + k * (kPanelB + 1)] * yk;
+        for (int i = k + 1 + threadIdx.x; i < w; i += 32) vs[i] -= D[i + k * (kSolveB + 1)] * yk;
         if (threadIdx.x == 0) vs[k] = yk;
         __syncwarp();
       }
@@ -616,12 +770,12 @@ __global__ void __launch_bounds__(256) k_fwd_large_diag(DevFronts F, const int32
 template <typename T>
 __global__ void __launch_bounds__(kSolveRows) k_fwd_large_gemv(DevFronts F, const int32_t* list, int step,
                                                                const T* __restrict__ panel, T* V, int nrhs) {
-  __shared__ T ys[kPanelB];
+  __shared__ T ys[kSolveB];
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nf = nc + F.nr[f];
-  const int c0 = step * kPanelB;
+  const int c0 = step * kSolveB;
   if (c0 >= nc) return;
-  const int w = min(kPanelB, nc - c0);
+  const int w = min(kSolveB, nc - c0);
   const int i = c0 + w + blockIdx.x * blockDim.x + threadIdx.x;
   if (c0 + w + blockIdx.x * blockDim.x >= nf) return;
   const T* P = panel + F.panel_off[f];
@@ -664,12 +818,12 @@ template <typename T>
 __global__ void __launch_bounds__(kSolveRows) k_bwd_large_gemvt(DevFronts F, const int32_t* list, int step,
                                                                 const T* __restrict__ panel, const T* V, T* scratch,
                                                                 int nrhs) {
-  __shared__ T part[kSolveRows / 32][kPanelB];
+  __shared__ T part[kSolveRows / 32][kSolveB];
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nf = nc + F.nr[f];
-  const int c0 = step * kPanelB;
+  const int c0 = step * kSolveB;
   if (c0 >= nc) return;
-  const int w = min(kPanelB, nc - c0);
+  const int w = min(kSolveB, nc - c0);
   const int rstart = c0 + w + blockIdx.x * blockDim.x;
   const int nchunks = (nf - c0 - w + kSolveRows - 1) / kSolveRows;
   if (rstart >= nf) return;
@@ -689,7 +843,7 @@ __global__ void __launch_bounds__(kSolveRows) k_bwd_large_gemvt(DevFronts F, con
     if (threadIdx.x < w) {
       T s = T(0);
       for (int q = 0; q < kSolveRows / 32; ++q) s += part[q][threadIdx.x];
-      scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + blockIdx.x) * kPanelB + threadIdx.x] = s;
+      scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + blockIdx.x) * kSolveB + threadIdx.x] = s;
     }
     __syncthreads();
   }
@@ -700,33 +854,33 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_bwd_large_diag(DevFronts F, const int32_t* list, int step,
                                                         const T* __restrict__ panel, T* V, const T* scratch,
                                                         int nrhs) {
-  __shared__ T D[kPanelB * (kPanelB + 1)];
-  __shared__ T ts[kPanelB];
+  __shared__ T D[kSolveB * (kSolveB + 1)];
+  __shared__ T ts[kSolveB];
   const int f = list[blockIdx.x];
   const int nc = F.nc[f], nf = nc + F.nr[f];
-  const int c0 = step * kPanelB;
+  const int c0 = step * kSolveB;
   if (c0 >= nc) return;
-  const int w = min(kPanelB, nc - c0);
+  const int w = min(kSolveB, nc - c0);
   const int nchunks = (nf - c0 - w + kSolveRows - 1) / kSolveRows;
   const T* P = panel + F.panel_off[f];
   for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
     int j = e / w, i = e - j * w;
-    if (i >= j) D[i + j * (kPanelB + 1)] = P[(c0 + i) + (size_t)(c0 + j) * nf];
+    if (i >= j) D[i + j * (kSolveB + 1)] = P[(c0 + i) + (size_t)(c0 + j) * nf];
   }
   for (int r = 0; r < nrhs; ++r) {
     T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
     __syncthreads();
     for (int k = threadIdx.x; k < w; k += blockDim.x) {
       T s = Vf[c0 + k];
-      for (int q = 0; q < nchunks; ++q) s -= scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + q) * kPanelB + k];
+      for (int q = 0; q < nchunks; ++q) s -= scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + q) * kSolveB + k];
       ts[k] = s;
     }
     __syncthreads();
     if (threadIdx.x < 32) {
       for (int k = w - 1; k >= 0; --k) {
-        T yk = ts[k] / D[k + k * (kPanelB + 1)];
+        T yk = ts[k] / D[k + k * (kSolveB + 1)];
         __syncwarp();
-        for (int m = threadIdx.x; m < k; m += 32) ts[m] -= D[k + m * (kPanelB + 1)] * yk;
+        for (int m = threadIdx.x; m < k; m += 32) ts[m] -= D[k + m * (kSolveB + 1)] * yk;
         if (threadIdx.x == 0) ts[k] = yk;
         __syncwarp();
       }
@@ -840,7 +994,8 @@ cudaError_t prepare_kernels() {
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t r) { if (r != cudaSuccess && e == cudaSuccess) e = r; };
   chk(opt_in(k_small_front<double>)); chk(opt_in(k_small_front<float>));
-  chk(opt_in(k_panel<double>)); chk(opt_in(k_panel<float>));
+  chk(opt_in(k_potrf<double>)); chk(opt_in(k_potrf<float>));
+  chk(opt_in(k_trsm_dmma)); chk(opt_in(k_trsm_simt<double>)); chk(opt_in(k_trsm_simt<float>));
   chk(opt_in(k_update_dmma));
   chk(opt_in(k_update_simt<double>)); chk(opt_in(k_update_simt<float>));
   chk(opt_in(k_fwd_small<double>)); chk(opt_in(k_fwd_small<float>));
@@ -878,10 +1033,10 @@ void launch_small_fronts(const DevFronts& F, const int32_t* list, int count, int
   k_small_front<T><<<count, 256, sm, st>>>(F, list, a, panel, upool, info);
 }
 template <typename T>
-void launch_zero_large(const DevFronts& F, const int32_t* list, int count, int64_t max_elems, T* panel, T* upool,
+void launch_zero_large(const DevFronts& F, const int32_t* list, int count, int64_t max_cols, T* panel, T* upool,
                        cudaStream_t st) {
   if (count <= 0) return;
-  dim3 grid(clamp_grid(ceil_div(max_elems, 256 * 4), 1024), count);
+  dim3 grid(clamp_grid(ceil_div(max_cols, 8), 512), count);
   k_zero_large<T><<<grid, 256, 0, st>>>(F, list, panel, upool);
 }
 template <typename T>
@@ -899,32 +1054,44 @@ void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int m
   k_extend_add<T><<<grid, 256, 0, st>>>(F, list, panel, upool);
 }
 template <typename T>
-void launch_panel(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
-                  T* diag_scratch, int32_t* info, cudaStream_t st) {
+void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
+                  cudaStream_t st) {
   if (count <= 0) return;
-  size_t sm = ((size_t)kPanelB * (kPanelB + 1) + kPanelB + (size_t)kPanelRows * (kPanelB + 1)) * sizeof(T);
-  set_smem(k_panel<T>, sm);
-  dim3 grid(std::max(1, row_blocks), count);
-  k_panel<T><<<grid, kPanelRows, sm, st>>>(F, list, step, panel, diag_scratch, info);
+  size_t sm = ((size_t)kFactB * (kFactB + 1) + kFactB) * sizeof(T);
+  k_potrf<T><<<count, 256, sm, st>>>(F, list, step, panel, linv, info);
 }
 template <typename T>
-void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles, T* panel, T* upool,
-                   const T* diag_scratch, int kind, cudaStream_t st) {
-  if (count <= 0) return;
-  dim3 grid(std::max(1, tiles), count);
+void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
+                 const T* linv, int kind, cudaStream_t st) {
+  if (count <= 0 || row_blocks <= 0) return;
+  dim3 grid(row_blocks, count);
   if constexpr (sizeof(T) == 8) {
     if (kind == 0) {
-      size_t sm = 2 * (size_t)kPanelB * kLdK * sizeof(double);
-      set_smem(k_update_dmma, sm);
-      k_update_dmma<<<grid, 128, sm, st>>>(F, list, step, reinterpret_cast<double*>(panel),
-                                           reinterpret_cast<double*>(upool),
-                                           reinterpret_cast<const double*>(diag_scratch));
+      size_t sm = ((size_t)kFactB * kTrLdA + (size_t)kFactB * kTrLdB) * sizeof(double);
+      k_trsm_dmma<<<grid, 256, sm, st>>>(F, list, step, reinterpret_cast<double*>(panel),
+                                         reinterpret_cast<const double*>(linv));
       return;
     }
   }
-  size_t sm = 2 * (size_t)kPanelB * (kTile + 4) * sizeof(T);
-  set_smem(k_update_simt<T>, sm);
-  k_update_simt<T><<<grid, 256, sm, st>>>(F, list, step, panel, upool, diag_scratch);
+  size_t sm = ((size_t)kFactB * (kTrRows + 4) + (size_t)kFactB * (kFactB + 4)) * sizeof(T);
+  k_trsm_simt<T><<<grid, 256, sm, st>>>(F, list, step, panel, linv);
+}
+template <typename T>
+void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, int tiles64, T* panel,
+                   T* upool, int kind, cudaStream_t st) {
+  if (count <= 0) return;
+  if constexpr (sizeof(T) == 8) {
+    if (kind == 0) {
+      if (tiles128 <= 0) return;
+      size_t sm = 2 * 2 * (size_t)kUK * kULD * sizeof(double);
+      k_update_dmma<<<dim3(tiles128, count), 256, sm, st>>>(F, list, step, reinterpret_cast<double*>(panel),
+                                                              reinterpret_cast<double*>(upool));
+      return;
+    }
+  }
+  if (tiles64 <= 0) return;
+  size_t sm = 2 * (size_t)kSimtK * (kSimtTile + 4) * sizeof(T);
+  k_update_simt<T><<<dim3(tiles64, count), 256, sm, st>>>(F, list, step, panel, upool);
 }
 
 template <typename T>
@@ -948,7 +1115,7 @@ void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int ma
                       T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st, int64_t* launches) {
   if (count <= 0) return;
   k_fwd_large_gather<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
-  int steps = ceil_div(max_nc, kPanelB);
+  int steps = ceil_div(max_nc, kSolveB);
   int chunks = std::max(1, ceil_div(max_nf, kSolveRows));
   for (int s = 0; s < steps; ++s) {
     k_fwd_large_diag<T><<<count, 256, 0, st>>>(F, list, s, panel, V, nrhs);
@@ -962,7 +1129,7 @@ void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int ma
                       T* X, int64_t ldx, T* V, T* scratch, int nrhs, cudaStream_t st, int64_t* launches) {
   if (count <= 0) return;
   k_bwd_large_gather<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
-  int steps = ceil_div(max_nc, kPanelB);
+  int steps = ceil_div(max_nc, kSolveB);
   int chunks = std::max(1, ceil_div(max_nf, kSolveRows));
   for (int s = steps - 1; s >= 0; --s) {
     k_bwd_large_gemvt<T><<<dim3(chunks, count), kSolveRows, 0, st>>>(F, list, s, panel, V, scratch, nrhs);
@@ -1016,9 +1183,9 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
   template void launch_assemble_large<T>(const DevFronts&, const int32_t*, int, int, const double*, T*,             \
                                          cudaStream_t);                                                            \
   template void launch_extend_add<T>(const DevFronts&, const int32_t*, int, int, T*, T*, cudaStream_t);             \
-  template void launch_panel<T>(const DevFronts&, const int32_t*, int, int, int, T*, T*, int32_t*, cudaStream_t);   \
-  template void launch_update<T>(const DevFronts&, const int32_t*, int, int, int, T*, T*, const T*, int,            \
-                                 cudaStream_t);                                                                    \
+  template void launch_potrf<T>(const DevFronts&, const int32_t*, int, int, T*, T*, int32_t*, cudaStream_t);       \
+  template void launch_trsm<T>(const DevFronts&, const int32_t*, int, int, int, T*, const T*, int, cudaStream_t);  \
+  template void launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t); \
   template void launch_fwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, T*, int,     \
                                     cudaStream_t);                                                                 \
   template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, int,         \

@@ -10,9 +10,11 @@
 
 namespace mfd {
 
-constexpr int kPanelB = 64;          // column panel of the blocked large-front factorization
-constexpr int kPanelRows = 128;      // rows per CTA in the panel TRSM
-constexpr int kTile = 64;            // trailing-update output tile
+constexpr int kFactB = 128;          // column panel of the blocked large-front factorization
+constexpr int kTrRowsH = 64;         // rows per CTA of the panel TRSM
+constexpr int kUpdTile = 128;        // trailing-update output tile (tensor path)
+constexpr int kUpdTileSimt = 64;     // trailing-update output tile (FMA path)
+constexpr int kSolveB = 64;          // column step of the large-front solves
 constexpr int kSolveRows = 256;      // rows per CTA in the large-front solve GEMV kernels
 
 // Opt every shared-memory-heavy kernel into the large dynamic shared memory
@@ -34,7 +36,7 @@ template <typename T>
 void launch_small_fronts(const DevFronts& F, const int32_t* list, int count, int nf_max, const double* a, T* panel,
                          T* upool, int32_t* info, cudaStream_t st);
 template <typename T>
-void launch_zero_large(const DevFronts& F, const int32_t* list, int count, int64_t max_elems, T* panel, T* upool,
+void launch_zero_large(const DevFronts& F, const int32_t* list, int count, int64_t max_cols, T* panel, T* upool,
                        cudaStream_t st);
 template <typename T>
 void launch_assemble_large(const DevFronts& F, const int32_t* list, int count, int max_entries, const double* a,
@@ -42,14 +44,19 @@ void launch_assemble_large(const DevFronts& F, const int32_t* list, int count, i
 template <typename T>
 void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int max_nr, T* panel, T* upool,
                        cudaStream_t st);
-// The factored diagonal block of each front goes to diag_scratch (count x 64 x 64)
-// and the update launch of the same step copies it into the panel.
+// Panel step s of the blocked large-front factorization (columns s*kFactB ..):
+//   potrf  : one CTA per front; L11 into the panel, L11^{-1} into linv (count x 128 x 128)
+//   trsm   : rows below the diagonal block, X <- X L11^{-T}   (kind 0: DMMA, 1: FMA)
+//   update : trailing lower triangle -= P P^T                  (kind 0: DMMA 128-tiles, 1: FMA 64-tiles)
 template <typename T>
-void launch_panel(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
-                  T* diag_scratch, int32_t* info, cudaStream_t st);
+void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
+                  cudaStream_t st);
 template <typename T>
-void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles, T* panel, T* upool,
-                   const T* diag_scratch, int kind, cudaStream_t st);
+void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
+                 const T* linv, int kind, cudaStream_t st);
+template <typename T>
+void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, int tiles64, T* panel,
+                   T* upool, int kind, cudaStream_t st);
 
 // ---- solves --------------------------------------------------------------------
 template <typename T>

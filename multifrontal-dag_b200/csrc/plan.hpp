@@ -44,13 +44,15 @@ struct LaunchList {          // a list of front ids in the device list pool
   int32_t off = 0, count = 0;
   int32_t param = 0;         // kernel-specific (size bin, grid extent, step, ...)
   int32_t param2 = 0;
+  int32_t param3 = 0;
 };
 
 struct LevelPlan {
   std::vector<LaunchList> small;     // fused one-CTA fronts, one list per size bin
   LaunchList large;                  // blocked fronts (sorted by nc descending)
   std::vector<LaunchList> ext_add;   // per child rank: children of large fronts
-  std::vector<LaunchList> steps;     // per panel step: prefix of `large`, param = row blocks, param2 = tiles
+  std::vector<LaunchList> steps;     // per panel step: prefix of `large`; param = TRSM row blocks,
+                                     // param2 = 128-tiles, param3 = 64-tiles of the trailing triangle
   std::vector<LaunchList> solve_steps;
   int32_t large_max_nf = 0;
   int64_t large_zero_elems = 0;

@@ -52,7 +52,7 @@ class KernelProfile(C.Structure):
 
 
 KERNEL_CLASSES = ["small_front", "zero", "assemble", "extend_add", "panel", "update", "solve_small", "solve_large",
-                  "other"]
+                  "other", "trsm"]
 
 
 class Stats(C.Structure):

@@ -187,6 +187,29 @@ int mfd_get_profile(mfd_handle *h, int32_t kind, mfd_kernel_profile *out);
 
 int mfd_destroy(mfd_handle *h);
 
+/* ---- dense fronts without allocation ------------------------------------------
+ * No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc -- code that owns all device memory through its own arena (e.g. a
+ * Fortran driver or framework that reserved HBM up front), or a latency-
+ * critical loop that must not take the allocator's lock.  Partially factors
+ * `count` dense fronts held in one caller-owned device buffer `fronts`: front i
+ * is an nf[i] x nc[i] column-major panel at element offset panel_off[i]
+ * (ld = nf[i], lower triangle used) and an (nf-nc) x (nf-nc) update matrix at
+ * update_off[i] (ld = nf-nc; ignored when nf == nc).  On return the panel holds
+ * the factor columns and the update matrix has the Schur complement subtracted;
+ * *info is 0 or the 1-based front column of the first non-positive pivot.
+ * Scratch: a static device array of MFD_NOALLOC_MAX_FRONTS x 128 x 128 doubles
+ * (1 MiB) plus small tables, held by every GPU that loads the library until the
+ * process exits; count > MFD_NOALLOC_MAX_FRONTS is rejected with MFD_E_ARG.
+ * The first call on a device looks up the array's device address and sets
+ * kernel attributes; make that first call before any stream capture.  All
+ * calls share the one array, so calls that overlap on the GPU (other streams,
+ * other host threads) race.  Host-synchronous on `stream` (NULL = default). */
+#define MFD_NOALLOC_MAX_FRONTS 8
+int mfd_factor_fronts_noalloc(double *fronts, int32_t count, const int64_t *panel_off, const int64_t *update_off,
+                              const int32_t *nf, const int32_t *nc, int32_t *info, void *stream);
+const char *mfd_noalloc_last_error(void);
+
 /* Last error text of this thread. */
 const char *mfd_last_error(void);
 

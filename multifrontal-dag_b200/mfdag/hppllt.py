@@ -66,7 +66,8 @@ class Stats(C.Structure):
 EXPORTS = [
     "mfd_default_options", "mfd_create", "mfd_create_batch", "mfd_analyze", "mfd_analyze_batch", "mfd_factorize",
     "mfd_solve", "mfd_factorize_solve", "mfd_get_stats", "mfd_get_index", "mfd_get_symbolic", "mfd_get_front_panel",
-    "mfd_destroy", "mfd_last_error", "mfd_set_profiling", "mfd_get_profile", "mfd_symbolic_analyze", "mfd_symbolic_view", "mfd_symbolic_free", "hppllt_init", "hppllt_set_precision", "hppllt_analyze", "hppllt_set_ordering",
+    "mfd_destroy", "mfd_last_error", "mfd_set_profiling", "mfd_get_profile", "mfd_factor_fronts_noalloc",
+    "mfd_noalloc_last_error", "mfd_symbolic_analyze", "mfd_symbolic_view", "mfd_symbolic_free", "hppllt_init", "hppllt_set_precision", "hppllt_analyze", "hppllt_set_ordering",
     "hppllt_factorize", "hppllt_solve", "hppllt_finalize", "hppllt_get_time_info", "hppllt_get_cost",
     "hppllt_get_nonzero", "hppllt_get_array_size",
 ]
@@ -109,6 +110,8 @@ def load(build_if_missing: bool = True):
     L.mfd_get_front_panel.restype = i64
     L.mfd_get_front_panel.argtypes = [vp, i32, i32, vp]
     L.mfd_destroy.argtypes = [vp]
+    L.mfd_factor_fronts_noalloc.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp]
+    L.mfd_noalloc_last_error.restype = C.c_char_p
     L.mfd_set_profiling.argtypes = [vp, i32]
     L.mfd_get_profile.argtypes = [vp, i32, C.POINTER(KernelProfile)]
     L.mfd_symbolic_analyze.argtypes = [C.POINTER(vp), i32, vp, vp, vp, i32]
@@ -320,6 +323,26 @@ class Solver:
         if rc < 0:
             _check(rc)
         return out[:n]
+
+
+NOALLOC_MAX_FRONTS = 8
+
+
+def factor_fronts_noalloc(fronts, panel_off, update_off, nf, nc, stream=None) -> int:
+    """Partial Cholesky of dense fronts held in one caller-owned device buffer
+    (a float64 CUDA tensor), without any device allocation (see
+    mfd_factor_fronts_noalloc in include/mfdag.h).  Returns info."""
+    L = load()
+    po = np.ascontiguousarray(panel_off, dtype=np.int64)
+    uo = np.ascontiguousarray(update_off, dtype=np.int64)
+    f = _i32(nf)
+    c = _i32(nc)
+    info = np.zeros(1, np.int32)
+    rc = L.mfd_factor_fronts_noalloc(_ptr(fronts), int(len(f)), po.ctypes.data, uo.ctypes.data, f.ctypes.data,
+                                     c.ctypes.data, info.ctypes.data, stream)
+    if rc != 0:
+        raise MfdError(rc, L.mfd_noalloc_last_error().decode())
+    return int(info[0])
 
 
 # index ids of mfd_get_index

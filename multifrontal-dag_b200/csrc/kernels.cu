@@ -273,78 +273,158 @@ __global__ void __launch_bounds__(256) k_extend_add(DevFronts F, const int32_t* 
 //   k_trsm  : the rows below, X <- A L11^{-T} = A (L11^{-1})^T, a GEMM with K = w
 //   k_update: trailing C(lower) -= P P^T with P the solved panel rows
 
+// Diagonal-block POTRF + inverse, one CTA per front, w <= 128.  The lower
+// triangle is split into 4x4 tiles (528 for w = 128) and each of the 544
+// threads keeps one tile in registers.  Cholesky: at pivot k the owners of tile
+// column k/4 publish column k into a double-buffered shared array, one barrier,
+// then every thread applies A -= c_k c_k^T / d_k to its tile (unscaled columns;
+// L(:,k) = c_k / sqrt(d_k) at the end).  Inverse: forward substitution on the
+// identity in place, one barrier per row (row j and column j published, row j's
+// 1/L_jj scaling deferred to step j+1).  L11 goes to the panel, L11^{-1} to linv.
+constexpr int kPotrfThreads = 544;
 template <typename T>
-__global__ void __launch_bounds__(256) k_potrf(DevFronts F, const int32_t* list, int step, T* panel, T* linv,
-                                               int32_t* info) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int B = kFactB, LDD = kFactB + 1;
-  T* D = reinterpret_cast<T*>(smem_raw);
-  T* piv = D + B * LDD;          // pivots of the unscaled elimination, then 1/L_jj of the inverse
+__global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const int32_t* list, int step, T* panel,
+                                                            T* linv, int32_t* info) {
+  constexpr int B = kFactB;
+  __shared__ T colbuf[2][B];
+  __shared__ T rowbuf[2][B];
+  __shared__ T piv[B];
+  __shared__ T rs[B];
   const int f = list[blockIdx.x];
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int c0 = step * B;
   if (c0 >= nc) return;
   const int w = min(B, nc - c0);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int tid = threadIdx.x;
+  const int nt = (w + 3) / 4, ntiles = nt * (nt + 1) / 2;
   T* P = panel + F.panel_off[f];
-  for (int j = warp; j < w; j += nw)
-    for (int i = j + lane; i < w; i += 32) D[i + j * LDD] = P[(c0 + i) + (size_t)(c0 + j) * nf];
-  __syncthreads();
-  // Cholesky with deferred column scaling: step k subtracts c_k c_k^T / d_k from
-  // the trailing triangle using the unscaled column c_k, so one barrier per
-  // column suffices; L(:,k) = c_k / sqrt(d_k) is applied afterwards.
+  const bool own = tid < ntiles;
+  int tr = 0, tc = 0;
+  if (own) {
+    tr = (int)((sqrtf(8.0f * (float)tid + 1.0f) - 1.0f) * 0.5f);
+    while ((tr + 1) * (tr + 2) / 2 <= tid) ++tr;
+    while (tr * (tr + 1) / 2 > tid) --tr;
+    tc = tid - tr * (tr + 1) / 2;
+  }
+  const int i0 = 4 * tr, j0 = 4 * tc;
+  T tl[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = i0 + u, j = j0 + v;
+      tl[u][v] = (own && i < w && j <= i) ? P[(c0 + i) + (size_t)(c0 + j) * nf] : T(0);
+    }
+  // ---- Cholesky, one barrier per pivot ----
   for (int k = 0; k < w; ++k) {
-    T d = D[k + k * LDD];
+    T* cb = colbuf[k & 1];
+    if (own && tc == (k >> 2)) {
+      const int kv = k & 3;           // explicit select keeps the tile in registers
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u;
+        const T val = kv == 0 ? tl[u][0] : (kv == 1 ? tl[u][1] : (kv == 2 ? tl[u][2] : tl[u][3]));
+        if (i >= k && i < w) cb[i] = val;
+      }
+    }
+    __syncthreads();
+    T d = cb[k];
     if (!(d > T(0))) {
       if (tid == 0) atomicMin(info, F.first[f] + c0 + k + 1);
       d = T(1);
     }
     if (tid == 0) piv[k] = d;
-    const T inv_d = T(1) / d;
-    for (int j = k + 1 + warp; j < w; j += nw) {
-      const T ljk = D[j + k * LDD] * inv_d;
-      for (int i = j + lane; i < w; i += 32) D[i + j * LDD] -= D[i + k * LDD] * ljk;
-    }
-    __syncthreads();
-  }
-  for (int j = warp; j < w; j += nw) {
-    const T sd = dev_sqrt<T>(piv[j]);
-    const T inv = T(1) / sd;
-    for (int i = j + lane; i < w; i += 32) {
-      T v = i == j ? sd : D[i + j * LDD] * inv;
-      D[i + j * LDD] = v;
-      P[(c0 + i) + (size_t)(c0 + j) * nf] = v;
+    if (own && i0 + 3 > k) {
+      const T inv = T(1) / d;
+      T ci[4], cj[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u;
+        ci[u] = (i > k && i < w) ? cb[i] : T(0);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int j = j0 + v;
+        cj[v] = (j > k && j < w) ? cb[j] * inv : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          if (j0 + v <= i0 + u) tl[u][v] -= ci[u] * cj[v];
     }
   }
   __syncthreads();
-  // in-place inverse of L11 by forward substitution on the identity, one row
-  // per step; the scaling of pivot row j by 1/L_jj is deferred to step j+1
-  // (no other thread reads row j after step j), so one barrier per row.
+  for (int j = tid; j < w; j += blockDim.x) rs[j] = T(1) / dev_sqrt<T>(piv[j]);
+  __syncthreads();
+  if (own) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int i = i0 + u, j = j0 + v;
+        if (i < w && j <= i) {
+          const T l = i == j ? dev_sqrt<T>(piv[j]) : tl[u][v] * rs[j];
+          tl[u][v] = l;
+          P[(c0 + i) + (size_t)(c0 + j) * nf] = l;
+        }
+      }
+  }
+  // ---- in-place inverse, one barrier per row ----
   for (int j = 0; j < w; ++j) {
-    const T r = T(1) / D[j + j * LDD];
-    if (tid == 0) piv[j] = r;
-    for (int i = j + 1 + warp; i < w; i += nw) {
-      const T lik = D[i + j * LDD] * r;
-      __syncwarp();
-      for (int jp = lane; jp < j; jp += 32) D[i + jp * LDD] -= lik * D[j + jp * LDD];
-      if (lane == 0) D[i + j * LDD] = -lik;
-    }
-    if (j >= 1) {
-      const T rp = piv[j - 1];
-      for (int jp = tid; jp < j - 1; jp += blockDim.x) D[(j - 1) + jp * LDD] *= rp;
-      if (tid == 0) D[(j - 1) + (j - 1) * LDD] = rp;
+    T* rb = rowbuf[j & 1];
+    T* cb = colbuf[j & 1];
+    if (own) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const int i = i0 + u, jj = j0 + v;
+          if (i == j && jj < j) rb[jj] = tl[u][v];
+          if (jj == j && i > j && i < w) cb[i] = tl[u][v];
+        }
     }
     __syncthreads();
+    if (own && i0 + 3 >= j - 1 && j0 <= j) {
+      const T r = rs[j];
+      const T rp = j >= 1 ? rs[j - 1] : T(0);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u;
+        const T lik = (i > j && i < w) ? cb[i] * r : T(0);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const int jp = j0 + v;
+          if (i > j && i < w && jp <= j) tl[u][v] = jp < j ? tl[u][v] - lik * rb[jp] : -lik;
+          if (j >= 1 && i == j - 1 && jp <= j - 1) tl[u][v] = jp == j - 1 ? rp : tl[u][v] * rp;
+        }
+      }
+    }
   }
-  {
-    const T rp = piv[w - 1];
-    for (int jp = tid; jp < w - 1; jp += blockDim.x) D[(w - 1) + jp * LDD] *= rp;
-    if (tid == 0) D[(w - 1) + (w - 1) * LDD] = rp;
+  if (own) {
+    const T rl = rs[w - 1];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int i = i0 + u, jp = j0 + v;
+        if (i == w - 1 && jp <= w - 1) tl[u][v] = jp == w - 1 ? rl : tl[u][v] * rl;
+      }
   }
-  __syncthreads();
   T* Li = linv + (size_t)blockIdx.x * B * B;          // column-major, ld = B, zero outside the lower w x w
-  for (int j = warp; j < B; j += nw)
-    for (int i = lane; i < B; i += 32) Li[i + j * B] = (i >= j && i < w && j < w) ? D[i + j * LDD] : T(0);
+  for (int e = tid; e < B * B; e += blockDim.x) {
+    const int i = e % B, j = e / B;
+    if (!(i < w && j < w && i >= j)) Li[e] = T(0);
+  }
+  if (own) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int i = i0 + u, j = j0 + v;
+        if (i < w && j <= i) Li[i + j * B] = tl[u][v];
+      }
+  }
 }
 
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc, bool valid) {
@@ -555,17 +635,38 @@ __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32
     }
     __syncthreads();
   }
-  double* U = upool + F.u_off[f];
+  // Epilogue: stage P_i P_j^T in shared memory (the operand buffers are free
+  // now), then read-modify-write the tile column by column with coalesced,
+  // batched loads (all loads of a batch are issued before its stores).
+  constexpr int LDC = kUT + 1;
+  double* Cs = sm;
 #pragma unroll
   for (int mi = 0; mi < 8; ++mi)
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        int gi = i0 + wm * 64 + mi * 8 + g;
-        int gj = j0 + wn * 32 + ni * 8 + 2 * q + e;
-        if (gi < nf && gj < nf && gi >= gj) *trailing_addr(P, U, nc, nr, nf, gi, gj) -= acc[mi][ni][e];
-      }
+      for (int e = 0; e < 2; ++e)
+        Cs[(wm * 64 + mi * 8 + g) + (wn * 32 + ni * 8 + 2 * q + e) * LDC] = acc[mi][ni][e];
+  __syncthreads();
+  double* U = upool + F.u_off[f];
+  constexpr int kBatch = 8;
+  for (int e0 = threadIdx.x; e0 < kUT * kUT; e0 += kBatch * 256) {
+    double* addr[kBatch];
+    double val[kBatch];
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int e = e0 + b * 256;
+      const int r = e % kUT, c = e / kUT;
+      const int gi = i0 + r, gj = j0 + c;
+      addr[b] = (e < kUT * kUT && gi < nf && gj < nf && gi >= gj) ? trailing_addr(P, U, nc, nr, nf, gi, gj) : nullptr;
+      val[b] = addr[b] ? *addr[b] : 0.0;
+    }
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int e = e0 + b * 256;
+      if (addr[b]) *addr[b] = val[b] - Cs[(e % kUT) + (e / kUT) * LDC];
+    }
+  }
 }
 
 // Trailing update on the FMA pipes (any T): 64x64 tiles, K in chunks of 64,
@@ -994,7 +1095,6 @@ cudaError_t prepare_kernels() {
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t r) { if (r != cudaSuccess && e == cudaSuccess) e = r; };
   chk(opt_in(k_small_front<double>)); chk(opt_in(k_small_front<float>));
-  chk(opt_in(k_potrf<double>)); chk(opt_in(k_potrf<float>));
   chk(opt_in(k_trsm_dmma)); chk(opt_in(k_trsm_simt<double>)); chk(opt_in(k_trsm_simt<float>));
   chk(opt_in(k_update_dmma));
   chk(opt_in(k_update_simt<double>)); chk(opt_in(k_update_simt<float>));
@@ -1057,8 +1157,7 @@ template <typename T>
 void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
                   cudaStream_t st) {
   if (count <= 0) return;
-  size_t sm = ((size_t)kFactB * (kFactB + 1) + kFactB) * sizeof(T);
-  k_potrf<T><<<count, 256, sm, st>>>(F, list, step, panel, linv, info);
+  k_potrf<T><<<count, kPotrfThreads, 0, st>>>(F, list, step, panel, linv, info);
 }
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,

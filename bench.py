@@ -46,7 +46,42 @@ WORKLOADS = {
                      make=lambda: P.diffusion3d(80, 2), precision=1, max_zero=1000),
     "diff3d80_fp64": dict(desc="3D variable-coefficient diffusion 80^3 (n=512,000), FP64",
                           make=lambda: P.diffusion3d(80, 2), precision=0, max_zero=1000),
+    "elast40": dict(desc="3D Q1 hex elasticity 40^3 elements, 3 dof/node, x=0 clamped (n=201,720), 64 RHS, FP64",
+                    make=lambda: P.elasticity3d(40, 4, 64), precision=0, max_zero=1000),
+    "elast40_fp32ir": dict(desc="3D Q1 hex elasticity 40^3 elements (n=201,720), 64 RHS, FP32 factor + FP64 refinement",
+                           make=lambda: P.elasticity3d(40, 4, 64), precision=1, max_zero=1000),
+    "batch2000": dict(desc="2,000 shifted 2D 5-point Laplacians, sides ~ randint[16,128], shift ~ U[0,0.1], seed 3, FP64",
+                      make=lambda: BatchProblem(P.laplace2d_batch(2000, 3)), precision=0, max_zero=100, batch=True),
+    "batch2000_fp32ir": dict(desc="2,000 shifted 2D 5-point Laplacians (seed 3), FP32 factor + FP64 refinement",
+                             make=lambda: BatchProblem(P.laplace2d_batch(2000, 3)), precision=1, max_zero=100,
+                             batch=True),
 }
+
+
+class BatchProblem:
+    """Many independent systems solved as one handle: values and right-hand
+    sides concatenated in system order."""
+
+    def __init__(self, systems):
+        self.systems = systems
+        self.count = len(systems)
+        self.n = int(sum(p.n for p in systems))
+        self.val = np.concatenate([p.val for p in systems])
+        self.rhs = np.concatenate([p.rhs for p in systems])
+
+    @property
+    def nnz(self) -> int:
+        return int(self.val.size)
+
+    def analyze(self, H, **opts):
+        return H.Solver.analyze_batch([(p.n, p.col, p.row, p.order) for p in self.systems], **opts)
+
+    def backward_error(self, x) -> float:
+        worst, off = 0.0, 0
+        for p in self.systems:
+            worst = max(worst, P.backward_error(p.n, p.col, p.row, p.val, x[off:off + p.n], p.rhs))
+            off += p.n
+        return worst
 
 
 def log(*a):
@@ -142,47 +177,93 @@ def ncu_traffic(workload: str, kernel: str):
 # ---------------------------------------------------------------------------
 # CPU baseline: the oracle (restatement of the reference's numeric phase)
 # ---------------------------------------------------------------------------
-def cpu_reference(prob, max_zero, steps, threads, nb=128):
+def cpu_reference(prob, max_zero, steps, threads, nb=128, nrhs_sample=1):
+    """Oracle factorization (tree-level parallel over ``threads``) and solves;
+    with several right-hand sides the first ``nrhs_sample`` are solved (the
+    reference solves one vector per call)."""
     from oracle import oracle as O
     blas = O.use_system_blas(True)
     o = O.Oracle.analyze(prob.n, prob.col, prob.row, nb=nb, max_zero=max_zero, order_perm=prob.order)
     cost = o.cost()
+    multi = prob.rhs.ndim == 2
+    k = min(nrhs_sample, prob.rhs.shape[1]) if multi else 1
     ft, st = [], []
-    x = None
+    bwd = 0.0
     for _ in range(steps):
         t0 = time.perf_counter()
         info = o.factorize(prob.val, nthreads=threads)
         t1 = time.perf_counter()
-        x = o.solve(prob.rhs)
+        xs = [o.solve(prob.rhs[:, j] if multi else prob.rhs) for j in range(k)]
         t2 = time.perf_counter()
         assert info == 0
         ft.append(t1 - t0)
         st.append(t2 - t1)
-    bwd = P.backward_error(prob.n, prob.col, prob.row, prob.val, x, prob.rhs)
-    return {"cost": cost, "factor_s": ft, "solve_s": st, "bwd": bwd, "blas": blas, "nb": nb}
+    for j, x in enumerate(xs):
+        b = prob.rhs[:, j] if multi else prob.rhs
+        bwd = max(bwd, P.backward_error(prob.n, prob.col, prob.row, prob.val, x, b))
+    return {"cost": cost, "factor_s": ft, "solve_s": st, "bwd": bwd, "blas": blas, "nb": nb, "rhs_timed": k}
+
+
+def cpu_reference_batch(bp, max_zero, threads, sample, nb=128):
+    """Oracle over a sample of the batch's systems, one system per host thread
+    (each system factored single-threaded, as independent jobs would be)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    blas = O.use_system_blas(True)
+    systems = bp.systems[:sample]
+    handles = [O.Oracle.analyze(p.n, p.col, p.row, nb=nb, max_zero=max_zero, order_perm=p.order) for p in systems]
+    cost = sum(o.cost() for o in handles)
+
+    def job(i):
+        o, p = handles[i], systems[i]
+        info = o.factorize(p.val, nthreads=1)
+        x = o.solve(p.rhs)
+        return info, P.backward_error(p.n, p.col, p.row, p.val, x, p.rhs)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        res = list(ex.map(job, range(len(systems))))
+    dt = time.perf_counter() - t0
+    assert all(r[0] == 0 for r in res)
+    return {"systems": len(systems), "seconds": dt, "systems_per_s": len(systems) / dt, "cost": cost,
+            "bwd": max(r[1] for r in res), "blas": blas, "nb": nb}
 
 
 def run_reference_arm(args, wl, prob):
+    """The reference's CPU numeric phase (restated in C, oracle/) on this
+    workload with all host threads; at most 5 timed steps, one full
+    factorization + solve each (a batch: the first 200 systems per step)."""
     threads = os.cpu_count() or 1
-    steps = max(1, args.steps)
+    steps = max(1, min(args.steps, 5))
     t0 = time.time()
-    r = cpu_reference(prob, wl["max_zero"], steps + 0, threads)
-    fs = statistics.mean(r["factor_s"])
-    value = r["cost"] / fs / 1e9
-    line = {
-        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": args.gpus,
-        "steps": steps, "warmup": 0, "ms_per_step": round(1e3 * (fs + statistics.mean(r["solve_s"])), 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wl["desc"], "max_zero": wl["max_zero"], "nb": r["nb"], "n": prob.n, "nnz": prob.nnz,
-                   "cost_flops": r["cost"], "ordering": "geometric nested dissection"},
-        "cpu_baseline": {"value": round(value, 3), "unit": "GFLOP/s", "cores": threads, "kind": "port",
-                         "sample": f"full numeric factorization + solve of the workload, {steps} step(s), "
-                                   f"tree-level parallel over {threads} threads, {'OpenBLAS' if r['blas'] else 'C loops'}"
-                                   f" tiles nb={r['nb']}"},
-        "e2e": {"value": round(value, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "solve_ms": round(1e3 * statistics.mean(r["solve_s"]), 3), "bwd_err": r["bwd"],
-        "wall_s": round(time.time() - t0, 1),
-    }
+    batch = bool(wl.get("batch"))
+    base = {"impl": "reference", "metric": METRIC, "n_gpus": args.gpus, "steps": steps, "warmup": 0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
+    if batch:
+        rs = [cpu_reference_batch(prob, wl["max_zero"], threads, sample=200) for _ in range(steps)]
+        secs = statistics.mean(r["seconds"] for r in rs)
+        value = rs[0]["systems"] / secs
+        unit = "systems/s"
+        sample = (f"factor + solve of the first {rs[0]['systems']} of {prob.count} systems per step, one system per "
+                  f"thread, {'OpenBLAS' if rs[0]['blas'] else 'C loops'} tiles nb={rs[0]['nb']}")
+        extra = {"ms_per_step": round(1e3 * secs, 3), "bwd_err": max(r["bwd"] for r in rs)}
+        cfg = {"workload": wl["desc"], "systems": prob.count, "max_zero": wl["max_zero"], "nb": rs[0]["nb"]}
+    else:
+        r = cpu_reference(prob, wl["max_zero"], steps, threads)
+        fs = statistics.mean(r["factor_s"])
+        value = r["cost"] / fs / 1e9
+        unit = "GFLOP/s"
+        sample = (f"full numeric factorization + solve of one RHS per step, tree-level parallel over {threads} "
+                  f"threads, {'OpenBLAS' if r['blas'] else 'C loops'} tiles nb={r['nb']}")
+        extra = {"ms_per_step": round(1e3 * (fs + statistics.mean(r["solve_s"])), 3),
+                 "solve_ms": round(1e3 * statistics.mean(r["solve_s"]), 3), "bwd_err": r["bwd"]}
+        cfg = {"workload": wl["desc"], "max_zero": wl["max_zero"], "nb": r["nb"], "n": prob.n, "nnz": prob.nnz,
+               "cost_flops": r["cost"], "ordering": "geometric nested dissection"}
+    line = dict(base, value=round(value, 3), unit=unit, config=cfg,
+                cpu_baseline={"value": round(value, 3), "unit": unit, "cores": threads, "kind": "port",
+                              "sample": sample},
+                e2e={"value": round(value, 3), "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                wall_s=round(time.time() - t0, 1), **extra)
     print(json.dumps(line), flush=True)
 
 
@@ -221,17 +302,21 @@ def main():
     from mfdag import hppllt as H
     device = local
     torch.cuda.set_device(device)
+    dev = f"cuda:{device}"
     prob = wl["make"]()
+    batch = bool(wl.get("batch"))
+    nrhs = 1 if prob.rhs.ndim == 1 else int(prob.rhs.shape[1])
+    opts = dict(max_zero=wl["max_zero"], nb=10, precision=wl["precision"], device=device)
     t0 = time.perf_counter()
-    s = H.Solver.analyze(prob.n, prob.col, prob.row, prob.order, max_zero=wl["max_zero"], nb=10,
-                         precision=wl["precision"], device=device)
+    s = prob.analyze(H, **opts) if batch else H.Solver.analyze(prob.n, prob.col, prob.row, prob.order, **opts)
     t_setup = time.perf_counter() - t0
     st = s.stats()
     cost = int(st.cost)
-    a_dev = torch.from_numpy(prob.val).to(f"cuda:{device}")
-    b_dev = torch.from_numpy(prob.rhs).to(f"cuda:{device}")
+    rhs_cm = np.ascontiguousarray(prob.rhs.T) if nrhs > 1 else prob.rhs      # column-major (n, nrhs)
+    a_dev = torch.from_numpy(prob.val).to(dev)
+    b_dev = torch.from_numpy(rhs_cm).to(dev)
     x_dev = torch.empty_like(b_dev)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")   # 256 MiB > L2
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MiB > L2
 
     def step():
         info = s.factorize(a_dev)
@@ -239,7 +324,7 @@ def main():
         f_ms = s.stats().factor_ms
         x_dev.copy_(b_dev)
         torch.cuda.synchronize(device)
-        rep, rc = s.solve(x_dev)
+        rep, rc = s.solve(x_dev, nrhs=nrhs)
         assert rc == 0, rc
         return f_ms, rep.time_ms, rep.backward_error, rep.iterations
 
@@ -262,38 +347,51 @@ def main():
         dist.barrier()
     clocks = clk.summary()
     f_mean, s_mean = statistics.mean(fms), statistics.mean(sms)
-    tvec = torch.tensor([f_mean, s_mean, wall], dtype=torch.float64, device=f"cuda:{device}")
+    tvec = torch.tensor([f_mean, s_mean, wall], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(tvec, op=dist.ReduceOp.MAX)
     f_max, s_max, wall_max = (float(v) for v in tvec.tolist())
-    value = world * cost / (f_max * 1e-3) / 1e9
+    gflops = world * cost / (f_max * 1e-3) / 1e9
+    if batch:
+        unit, value = "systems/s", world * prob.count / ((f_max + s_max) * 1e-3)
+    else:
+        unit, value = "GFLOP/s", gflops
     st = s.stats()
     launches = args.steps * (int(st.launches_factor) + int(st.launches_solve) * max(1, max(its) if its else 1))
+    # host-side check of the last solution
+    x_last = x_dev.cpu().numpy()
+    x_last = x_last.T if nrhs > 1 else x_last
+    if batch:
+        host_bwd = prob.backward_error(x_last)
+    else:
+        host_bwd = P.backward_error(prob.n, prob.col, prob.row, prob.val, x_last, prob.rhs)
 
     # ---- end to end through the C ABI with host buffers (pinned) ----
     a_pin = torch.from_numpy(prob.val).pin_memory()
-    b_host = torch.from_numpy(prob.rhs.copy()).pin_memory()
+    b_host = torch.from_numpy(rhs_cm.copy()).pin_memory()
     e2e_t = []
     for k in range(args.steps + 1):
         x_host = b_host.clone()
         t0 = time.perf_counter()
         info = s.factorize(a_pin)
-        rep, rc = s.solve(x_host)
+        rep, rc = s.solve(x_host, nrhs=nrhs)
         t1 = time.perf_counter()
         assert info == 0 and rc == 0
         if k > 0:
             e2e_t.append(t1 - t0)
-    e2e_tv = torch.tensor([statistics.mean(e2e_t)], dtype=torch.float64, device=f"cuda:{device}")
+    e2e_tv = torch.tensor([statistics.mean(e2e_t)], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(e2e_tv, op=dist.ReduceOp.MAX)
-    e2e_value = world * cost / float(e2e_tv.item()) / 1e9
+    e2e_s = float(e2e_tv.item())
+    e2e_value = world * prob.count / e2e_s if batch else world * cost / e2e_s / 1e9
 
     # ---- roofline of the dominant kernel (per-launch events, graphs off) ----
     roof = None
     prof = None
+    nprof = max(1, min(args.steps, 3))
     if not args.no_profile:
         s.set_profiling(True)
-        for _ in range(max(1, min(args.steps, 3))):
+        for _ in range(nprof):
             step()
         prof = s.profile()
         s.set_profiling(False)
@@ -307,6 +405,10 @@ def main():
             roof = {"kernel": dom, "bound": "tensor", "achieved": round(d["flops"] / (d["ms"] * 1e-3) / 1e12, 3),
                     "peak": round(peak, 3), "unit": "TFLOP/s",
                     "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)"}
+        elif dom in ("update", "trsm"):
+            peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops", 1400.0)))
+            roof = {"kernel": dom, "bound": "tensor", "achieved": round(d["flops"] / (d["ms"] * 1e-3) / 1e12, 3),
+                    "peak": peak, "unit": "TFLOP/s", "peak_source": "MEASURED_PEAKS.json bf16 (sustained)"}
         else:
             peak = float(peaks.get("hbm_gbs", 6650.0))
             roof = {"kernel": dom, "bound": "hbm", "achieved": round(d["bytes"] / (d["ms"] * 1e-3) / 1e9, 1),
@@ -314,8 +416,9 @@ def main():
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
         roof["frac"] = round(roof["achieved"] / roof["peak"], 4)
         roof["traffic"] = ncu_traffic(args.workload, dom)
-        roof["launches_per_step"] = d["launches"] // max(1, min(args.steps, 3))
+        roof["launches_per_step"] = d["launches"] // nprof
         roof["avg_launch_ms"] = round(per_launch_ms, 4)
+        roof["algorithmic_per_launch"] = (d["flops"] if roof["bound"] == "tensor" else d["bytes"]) / max(1, d["launches"])
         roof["share_of_factor"] = round(d["ms"] / max(1e-9, sum(prof[k]["ms"] for k in fact_classes)), 3)
 
     # ---- CPU baseline (rank 0, N = 1) ----
@@ -323,41 +426,52 @@ def main():
     if rank == 0 and world == 1 and args.cpu_baseline == "auto":
         threads = os.cpu_count() or 1
         try:
-            r = cpu_reference(prob, wl["max_zero"], 1, threads)
-            fs = r["factor_s"][0]
-            cpu = {"value": round(r["cost"] / fs / 1e9, 3), "unit": "GFLOP/s", "cores": threads, "kind": "port",
-                   "sample": f"one full numeric factorization of the same workload (oracle, tree-level parallel, "
-                             f"{'OpenBLAS' if r['blas'] else 'C loops'} tiles nb={r['nb']}), {fs:.1f} s",
-                   "solve_ms": round(1e3 * r["solve_s"][0], 2), "bwd_err": r["bwd"]}
+            if batch:
+                r = cpu_reference_batch(prob, wl["max_zero"], threads, sample=200)
+                cpu = {"value": round(r["systems_per_s"], 3), "unit": "systems/s", "cores": threads, "kind": "port",
+                       "sample": f"factor + solve of the first {r['systems']} of the {prob.count} systems, one system "
+                                 f"per thread (oracle, {'OpenBLAS' if r['blas'] else 'C loops'} tiles nb={r['nb']}), "
+                                 f"{r['seconds']:.1f} s", "bwd_err": r["bwd"]}
+            else:
+                r = cpu_reference(prob, wl["max_zero"], 1, threads, nrhs_sample=min(nrhs, 2))
+                fs = r["factor_s"][0]
+                cpu = {"value": round(r["cost"] / fs / 1e9, 3), "unit": "GFLOP/s", "cores": threads, "kind": "port",
+                       "sample": f"one full numeric factorization of the same workload (oracle, tree-level parallel, "
+                                 f"{'OpenBLAS' if r['blas'] else 'C loops'} tiles nb={r['nb']}), {fs:.1f} s"
+                                 + (f"; solve of {r['rhs_timed']} of {nrhs} RHS, scaled" if nrhs > 1 else ""),
+                       "solve_ms": round(1e3 * r["solve_s"][0] * nrhs / r["rhs_timed"], 2), "bwd_err": r["bwd"]}
         except Exception as e:  # noqa: BLE001
-            cpu = {"value": None, "unit": "GFLOP/s", "cores": threads, "kind": "port", "sample": f"failed: {e}"}
+            cpu = {"value": None, "unit": unit, "cores": threads, "kind": "port", "sample": f"failed: {e}"}
 
     if rank == 0:
+        cfg = {"workload": wl["desc"], "name": args.workload, "n": prob.n, "nnz_lower": prob.nnz, "nrhs": nrhs,
+               "fronts": int(st.num_front), "levels": int(st.num_level), "max_front": int(st.max_front),
+               "cost_flops": cost, "nnz_L": int(st.nonzero), "nb": 10, "max_zero": wl["max_zero"],
+               "ordering": "geometric nested dissection",
+               "l2": "flushed (256 MiB write) between timed steps; working set > L2",
+               "parallelism": f"{world} independent replica(s)"}
+        if batch:
+            cfg["systems"] = prob.count
+        h2d = int(8 * prob.nnz + 8 * prob.n * nrhs)
         line = {
-            "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC, "value": round(value, 3), "unit": unit, "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": round(f_max + s_max, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if wl["precision"] == 0 else "f32+f64ir",
-            "data": "synthetic",
-            "config": {"workload": wl["desc"], "name": args.workload, "n": prob.n, "nnz_lower": prob.nnz,
-                       "fronts": int(st.num_front), "levels": int(st.num_level), "max_front": int(st.max_front),
-                       "cost_flops": cost, "nnz_L": int(st.nonzero), "nb": 10, "max_zero": wl["max_zero"],
-                       "ordering": "geometric nested dissection",
-                       "l2": "flushed (256 MiB write) between timed steps; working set > L2",
-                       "parallelism": f"{world} independent replica(s)"},
-            "factor_ms": round(f_max, 3), "solve_ms": round(s_max, 3), "bwd_err": max(bwds),
+            "data": "synthetic", "config": cfg,
+            "factor_ms": round(f_max, 3), "factor_gflops": round(gflops, 3), "solve_ms": round(s_max, 3),
+            "bwd_err": max(bwds), "bwd_err_host": host_bwd,
             "ir_iterations": max(its) if its else 0, "wall_ms_per_step": round(1e3 * wall_max / args.steps, 3),
             "setup_s": round(t_setup, 2),
             "clocks": clocks,
-            "e2e": {"value": round(e2e_value, 3), "unit": "GFLOP/s",
-                    "h2d_bytes_per_step": int(8 * prob.nnz + 8 * prob.n), "d2h_bytes_per_step": int(8 * prob.n + 4),
+            "e2e": {"value": round(e2e_value, 3), "unit": unit, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": int(8 * prob.n * nrhs + 4), "ms_per_step": round(1e3 * e2e_s, 3),
                     "what": "mfd_factorize(pinned host A) + mfd_solve(pinned host b), wall clock"},
             "gpu_launches": launches,
             "roofline": roof,
             "cpu_baseline": cpu,
         }
         if prof is not None:
-            line["kernel_profile_ms_per_step"] = {k: round(v["ms"] / max(1, min(args.steps, 3)), 3)
-                                                  for k, v in prof.items() if v["launches"]}
+            line["kernel_profile_ms_per_step"] = {k: round(v["ms"] / nprof, 3) for k, v in prof.items() if v["launches"]}
         print(json.dumps(line), flush=True)
     s.close()
     if world > 1:

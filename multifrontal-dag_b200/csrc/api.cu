@@ -66,17 +66,43 @@ struct DBuf {
   }
 };
 
-// first-fit allocator over a simulated address space (static memory plan)
-struct FirstFit {
-  std::map<int64_t, int64_t> free_;  // offset -> size
+// best-fit allocator over a simulated address space (static memory plan):
+// free blocks indexed by address (for coalescing) and by size (for the
+// search), so a plan over millions of fronts stays O(F log F)
+struct BestFit {
+  std::map<int64_t, int64_t> by_addr;            // offset -> size
+  std::multimap<int64_t, int64_t> by_size;       // size -> offset
   int64_t top = 0;
+  void erase_size(int64_t size, int64_t off) {
+    auto r = by_size.equal_range(size);
+    for (auto it = r.first; it != r.second; ++it)
+      if (it->second == off) {
+        by_size.erase(it);
+        return;
+      }
+  }
+  void insert(int64_t off, int64_t size) {
+    by_addr[off] = size;
+    by_size.emplace(size, off);
+  }
   int64_t alloc(int64_t size) {
     size = align_up(std::max<int64_t>(size, 1));
-    for (auto it = free_.begin(); it != free_.end(); ++it) {
-      if (it->second >= size) {
-        int64_t off = it->first, rest = it->second - size;
-        free_.erase(it);
-        if (rest > 0) free_[off + size] = rest;
+    auto it = by_size.lower_bound(size);
+    if (it != by_size.end()) {
+      int64_t off = it->second, have = it->first;
+      by_size.erase(it);
+      by_addr.erase(off);
+      if (have > size) insert(off + size, have - size);
+      return off;
+    }
+    // extend the top, reusing a free block that ends there
+    if (!by_addr.empty()) {
+      auto last = std::prev(by_addr.end());
+      if (last->first + last->second == top) {
+        int64_t off = last->first;
+        erase_size(last->second, off);
+        by_addr.erase(last);
+        top = off + size;
         return off;
       }
     }
@@ -86,19 +112,22 @@ struct FirstFit {
   }
   void release(int64_t off, int64_t size) {
     size = align_up(std::max<int64_t>(size, 1));
-    auto it = free_.emplace(off, size).first;
-    auto nx = std::next(it);
-    if (nx != free_.end() && it->first + it->second == nx->first) {
-      it->second += nx->second;
-      free_.erase(nx);
+    auto nx = by_addr.lower_bound(off);
+    if (nx != by_addr.end() && off + size == nx->first) {
+      size += nx->second;
+      erase_size(nx->second, nx->first);
+      nx = by_addr.erase(nx);
     }
-    if (it != free_.begin()) {
-      auto pv = std::prev(it);
-      if (pv->first + pv->second == it->first) {
-        pv->second += it->second;
-        free_.erase(it);
+    if (nx != by_addr.begin()) {
+      auto pv = std::prev(nx);
+      if (pv->first + pv->second == off) {
+        off = pv->first;
+        size += pv->second;
+        erase_size(pv->second, pv->first);
+        by_addr.erase(pv);
       }
     }
+    insert(off, size);
   }
 };
 
@@ -282,11 +311,11 @@ int build_plan(mfd_handle* h) {
     fr.s_off = h->s_elems;
     if (nf > sfm) h->s_elems += (int64_t)((nf + kSolveRows - 1) / kSolveRows) * kSolveB;
   }
-  // update pool: static first-fit plan over level lifetimes
+  // update pool: static best-fit plan over level lifetimes
   {
     std::vector<std::vector<int32_t>> by_level(nlev);
     for (int32_t g = 0; g < nfr; ++g) by_level[h->fronts[g].level].push_back(g);
-    FirstFit ff;
+    BestFit ff;
     for (int l = 0; l < nlev; ++l) {
       for (int32_t g : by_level[l]) {
         int64_t nr = h->fronts[g].nr;

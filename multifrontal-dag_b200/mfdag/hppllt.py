@@ -265,15 +265,26 @@ class Solver:
         _check(rc)
         return 0
 
-    def solve(self, b, report: bool = True):
-        """Solve in place; b is (n,) or (n, nrhs) Fortran-ordered numpy, or a CUDA tensor."""
+    def solve(self, b, report: bool = True, nrhs: int | None = None):
+        """Solve in place.  b holds nrhs column-major right-hand sides of length
+        n: a numpy array (n,) or Fortran-ordered (n, nrhs), or a float64 tensor
+        (host or CUDA) whose storage is that column-major block -- a contiguous
+        (nrhs, n) tensor, or (n,) with nrhs = 1.  ``nrhs`` overrides the count
+        read from the shape."""
         rep = Report()
         if isinstance(b, np.ndarray):
             if b.dtype != np.float64 or not (b.flags.f_contiguous or b.ndim == 1):
                 raise ValueError("b must be float64, 1-D or Fortran ordered")
-            nrhs = 1 if b.ndim == 1 else b.shape[1]
+            k = 1 if b.ndim == 1 else b.shape[1]
+            size = b.size
         else:
-            nrhs = 1 if b.dim() == 1 else b.shape[1]
+            if not b.is_contiguous():
+                raise ValueError("tensor right-hand sides must be contiguous (nrhs, n) storage")
+            k = 1 if b.dim() == 1 else (b.shape[0] if b.shape[-1] == self.n else b.shape[1])
+            size = b.numel()
+        nrhs = k if nrhs is None else int(nrhs)
+        if nrhs < 1 or size != nrhs * self.n:
+            raise ValueError(f"right-hand side holds {size} values, expected {nrhs} x {self.n}")
         rc = load().mfd_solve(self._h, _ptr(b), int(nrhs), int(self.n), C.byref(rep) if report else None)
         if rc not in (0, -5):
             _check(rc)

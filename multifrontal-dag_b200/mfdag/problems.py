@@ -206,12 +206,28 @@ def diffusion3d(side: int = 80, seed: int = 2, nd: bool = True) -> Problem:
     return Problem(f"diffusion3d_{side}^3", n, ptr, row, val, order, b, x, {"dims": dims})
 
 
+_GRID2D_CACHE: dict = {}
+
+
+def _grid2d(side: int, nd: bool):
+    """5-point structure, unshifted values and ordering of one side (memoized:
+    a 2,000-system batch has at most 113 distinct sides)."""
+    key = (side, nd)
+    if key not in _GRID2D_CACHE:
+        ptr, row, val = grid_laplacian((side, side), diag=4.0)
+        order = nested_dissection((side, side)) if nd else None
+        diag_pos = (ptr[:-1] - 1).astype(np.int64)        # the diagonal leads each column
+        _GRID2D_CACHE[key] = (ptr, row, val, order, diag_pos)
+    return _GRID2D_CACHE[key]
+
+
 def laplace2d_batch(count: int = 2000, seed: int = 3, lo: int = 16, hi: int = 128, nd: bool = True):
     """Uneven batch of shifted 2D 5-point Laplacians.
 
     From one generator seeded with ``seed``: sides ~ randint[lo, hi] (inclusive),
     then shifts ~ U[0, 0.1], then each system's RHS ~ U[-1, 1] in system order.
-    A_i = 5-point(s_i) + shift_i I.
+    A_i = 5-point(s_i) + shift_i I.  Systems of equal side share their
+    structure and ordering arrays (read-only).
     """
     rng = np.random.default_rng(seed)
     sides = rng.integers(lo, hi + 1, size=count)
@@ -219,12 +235,98 @@ def laplace2d_batch(count: int = 2000, seed: int = 3, lo: int = 16, hi: int = 12
     out = []
     for i in range(count):
         s = int(sides[i])
-        ptr, row, val = grid_laplacian((s, s), diag=4.0, shift=float(shifts[i]))
+        ptr, row, val0, order, diag_pos = _grid2d(s, nd)
+        val = val0.copy()
+        val[diag_pos] += float(shifts[i])
         b = rng.uniform(-1.0, 1.0, s * s)
-        order = nested_dissection((s, s)) if nd else None
         out.append(Problem(f"batch_{i}_{s}", s * s, ptr, row, val, order, b, None,
                            {"dims": (s, s), "shift": float(shifts[i])}))
     return out
+
+
+def _hex_stiffness_parts():
+    """Q1 (trilinear) hexahedron on the unit cube, 2x2x2 Gauss quadrature.
+
+    Returns (K_lambda, K_mu), 24 x 24, such that an isotropic element's
+    stiffness is lambda * K_lambda + mu * K_mu.  Local nodes are the cube's
+    corners in lexicographic order (x fastest), dofs node-major (ux, uy, uz).
+    Strain rows: xx, yy, zz, xy, yz, zx (engineering shear).
+    """
+    corners = np.array([[a, b, c] for c in (0, 1) for b in (0, 1) for a in (0, 1)], dtype=np.float64)
+    gp = np.array([0.5 - 0.5 / np.sqrt(3.0), 0.5 + 0.5 / np.sqrt(3.0)])
+    m = np.array([1.0, 1.0, 1.0, 0.0, 0.0, 0.0])
+    Dl = np.outer(m, m)
+    Dm = np.diag([2.0, 2.0, 2.0, 1.0, 1.0, 1.0])
+    Kl = np.zeros((24, 24))
+    Km = np.zeros((24, 24))
+    for z in gp:
+        for y in gp:
+            for x in gp:
+                pt = (x, y, z)
+                lin = np.where(corners == 1.0, np.array(pt)[None, :], 1.0 - np.array(pt)[None, :])   # 8 x 3 factors
+                sgn = np.where(corners == 1.0, 1.0, -1.0)
+                grad = np.empty((8, 3))
+                for d in range(3):
+                    others = [e for e in range(3) if e != d]
+                    grad[:, d] = sgn[:, d] * lin[:, others[0]] * lin[:, others[1]]
+                B = np.zeros((6, 24))
+                for k in range(8):
+                    gx, gy, gz = grad[k]
+                    c = 3 * k
+                    B[0, c] = gx
+                    B[1, c + 1] = gy
+                    B[2, c + 2] = gz
+                    B[3, c], B[3, c + 1] = gy, gx
+                    B[4, c + 1], B[4, c + 2] = gz, gy
+                    B[5, c], B[5, c + 2] = gz, gx
+                w = 1.0 / 8.0
+                Kl += w * B.T @ Dl @ B
+                Km += w * B.T @ Dm @ B
+    return Kl, Km
+
+
+def elasticity3d(ne: int = 40, seed: int = 4, nrhs: int = 64, nd: bool = True) -> Problem:
+    """3D linear elasticity, Q1 hexahedra on an ne^3 unit-element mesh, 3 dofs
+    per node, the face x = 0 clamped (its nodes removed).
+
+    From one generator seeded with ``seed``, per element (x fastest):
+    E = 10^U[-1, 1], then nu ~ U[0.25, 0.35]; then the nrhs right-hand sides
+    ~ U[-1, 1] as an (n, nrhs) Fortran-ordered array.  Free nodes are the
+    (ne) x (ne+1) x (ne+1) grid x = 1..ne, numbered x fastest, dofs node-major.
+    """
+    import scipy.sparse as sp
+    rng = np.random.default_rng(seed)
+    nel = ne ** 3
+    E = 10.0 ** rng.uniform(-1.0, 1.0, nel)
+    nu = rng.uniform(0.25, 0.35, nel)
+    lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+    mu = E / (2.0 * (1.0 + nu))
+    Kl, Km = _hex_stiffness_parts()
+    nx, ny, nz = ne, ne + 1, ne + 1               # free-node grid
+    n = 3 * nx * ny * nz
+    e = np.arange(nel)
+    ex, ey, ez = e % ne, (e // ne) % ne, e // (ne * ne)
+    corners = [(a, b, c) for c in (0, 1) for b in (0, 1) for a in (0, 1)]
+    gd = np.empty((nel, 24), dtype=np.int64)
+    for k, (a, b, c) in enumerate(corners):
+        x = ex + a
+        node = (x - 1) + nx * ((ey + b) + ny * (ez + c))
+        for d in range(3):
+            gd[:, 3 * k + d] = np.where(x >= 1, 3 * node + d, -1)
+    r = np.repeat(gd, 24, axis=1).reshape(nel, 24, 24)
+    cidx = np.tile(gd, (1, 24)).reshape(nel, 24, 24)
+    keep = (r >= cidx) & (cidx >= 0)
+    vals = (lam[:, None, None] * Kl[None] + mu[:, None, None] * Km[None])[keep]
+    A = sp.coo_matrix((vals, (r[keep], cidx[keep])), shape=(n, n)).tocsc()
+    A.sum_duplicates()
+    A.sort_indices()
+    ptr = (A.indptr + 1).astype(np.int32)
+    row = (A.indices + 1).astype(np.int32)
+    val = A.data.astype(np.float64)
+    b = np.asfortranarray(rng.uniform(-1.0, 1.0, (n, nrhs)))
+    order = nested_dissection((nx, ny, nz), dof=3) if nd else None
+    return Problem(f"elasticity3d_{ne}^3", n, ptr, row, val, order, b, None,
+                   {"dims": (nx, ny, nz), "dof": 3, "elements": nel})
 
 
 def backward_error(n, ptr, row, val, x, b) -> float:

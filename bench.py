@@ -165,11 +165,17 @@ def fp64_gemm_peak(torch, device) -> float:
     return best
 
 
-def ncu_traffic(workload: str, kernel: str):
-    """DRAM bytes per launch from a committed ncu summary, if one exists."""
+def ncu_traffic(workload: str, kernel: str, alg_bytes_per_launch: float):
+    """DRAM bytes per launch: the committed ncu ratio (DRAM bytes per
+    algorithmic byte, profiles/ncu_traffic.json) times this run's average
+    algorithmic bytes per launch; None without a capture for the kernel."""
     try:
         d = json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic.json")))
-        return d.get(workload, {}).get(kernel)
+        e = d.get(workload, {}).get(kernel)
+        if not e:
+            return None
+        return {"bytes_per_launch": round(e["dram_per_alg_byte"] * alg_bytes_per_launch),
+                "dram_per_alg_byte": e["dram_per_alg_byte"], "source": e["source"]}
     except Exception:
         return None
 
@@ -415,7 +421,9 @@ def main():
                     "peak": peak, "unit": "GB/s",
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
         roof["frac"] = round(roof["achieved"] / roof["peak"], 4)
-        roof["traffic"] = ncu_traffic(args.workload, dom)
+        tr = ncu_traffic(args.workload, dom, d["bytes"] / max(1, d["launches"]))
+        roof["traffic"] = tr["bytes_per_launch"] if tr else None
+        roof["traffic_source"] = tr if tr else "no ncu capture committed for this kernel and workload"
         roof["launches_per_step"] = d["launches"] // nprof
         roof["avg_launch_ms"] = round(per_launch_ms, 4)
         roof["algorithmic_per_launch"] = (d["flops"] if roof["bound"] == "tensor" else d["bytes"]) / max(1, d["launches"])

@@ -159,14 +159,14 @@ struct mfd_handle {
   std::vector<LevelPlan> levels;
   std::vector<int32_t> h_lists;
   std::vector<int> small_bins;
-  int64_t panel_elems = 0, upool_elems = 0, v_elems = 0, s_elems = 0;
+  int64_t panel_elems = 0, upool_elems = 0, v_elems = 0, s_elems = 0, dinv_elems = 0;
   int32_t max_large_count = 0, max_nf = 0;
   int64_t cost = 0, nonzero = 0;
 
   // device tables
   DBuf<int32_t> d_nc, d_nr, d_first, d_parent, d_child_ptr, d_child, d_lrow_off, d_lrow, d_local, d_a_beg, d_a_src,
       d_a_pos, d_sidx, d_lists, d_perm, d_info;
-  DBuf<int64_t> d_panel_off, d_u_off, d_v_off, d_s_off;
+  DBuf<int64_t> d_panel_off, d_u_off, d_v_off, d_s_off, d_d_off;
   DevFronts F{};
 
   // CSR of the permuted full matrix (residuals)
@@ -298,7 +298,7 @@ int build_plan(mfd_handle* h) {
   }
   // panel offsets, solve vector offsets, large-front solve scratch
   const int sfm = small_front_max(h);
-  h->panel_elems = h->v_elems = h->s_elems = 0;
+  h->panel_elems = h->v_elems = h->s_elems = h->dinv_elems = 0;
   h->max_nf = 0;
   for (int32_t g = 0; g < nfr; ++g) {
     HostFront& fr = h->fronts[g];
@@ -309,7 +309,11 @@ int build_plan(mfd_handle* h) {
     fr.v_off = h->v_elems;
     h->v_elems += nf;
     fr.s_off = h->s_elems;
-    if (nf > sfm) h->s_elems += (int64_t)((nf + kSolveRows - 1) / kSolveRows) * kSolveB;
+    fr.d_off = h->dinv_elems;
+    if (nf > sfm) {
+      h->s_elems += (int64_t)((nf + kSolveRows - 1) / kSolveRows) * kSolveB;
+      h->dinv_elems += (int64_t)((fr.nc + kFactB - 1) / kFactB) * kFactB * kFactB;   // kept for the solves
+    }
   }
   // update pool: static best-fit plan over level lifetimes
   {
@@ -430,11 +434,11 @@ int upload_plan(mfd_handle* h) {
   cudaStream_t st = h->st;
   const int32_t nfr = h->num_front;
   std::vector<int32_t> nc(nfr), nr(nfr), first(nfr), parent(nfr);
-  std::vector<int64_t> poff(nfr), uoff(nfr), voff(nfr), soff(nfr);
+  std::vector<int64_t> poff(nfr), uoff(nfr), voff(nfr), soff(nfr), doff(nfr);
   for (int32_t g = 0; g < nfr; ++g) {
     const HostFront& f = h->fronts[g];
     nc[g] = f.nc; nr[g] = f.nr; first[g] = f.first; parent[g] = f.parent;
-    poff[g] = f.panel_off; uoff[g] = f.u_off; voff[g] = f.v_off; soff[g] = f.s_off;
+    poff[g] = f.panel_off; uoff[g] = f.u_off; voff[g] = f.v_off; soff[g] = f.s_off; doff[g] = f.d_off;
   }
   std::vector<int32_t> lrow_glob;
   lrow_glob.reserve(h->h_lrow_off[nfr]);
@@ -454,6 +458,7 @@ int upload_plan(mfd_handle* h) {
   CK(h->d_u_off.upload(uoff, st));
   CK(h->d_v_off.upload(voff, st));
   CK(h->d_s_off.upload(soff, st));
+  CK(h->d_d_off.upload(doff, st));
   CK(h->d_lists.upload(h->h_lists, st));
   CK(h->d_a_src.alloc(h->nnz_total));
   CK(h->d_a_pos.alloc(h->nnz_total));
@@ -464,6 +469,7 @@ int upload_plan(mfd_handle* h) {
   F.child_ptr = h->d_child_ptr.p; F.child = h->d_child.p; F.panel_off = h->d_panel_off.p; F.u_off = h->d_u_off.p;
   F.lrow_off = h->d_lrow_off.p; F.lrow = h->d_lrow.p; F.local = h->d_local.p; F.a_beg = h->d_a_beg.p;
   F.a_src = h->d_a_src.p; F.a_pos = h->d_a_pos.p; F.v_off = h->d_v_off.p; F.s_off = h->d_s_off.p;
+  F.d_off = h->d_d_off.p;
 
   // permuted global A structure, value sources, front of every column
   std::vector<int32_t> acol(h->n_total + 1), arow(h->nnz_total), src(h->nnz_total), colf(h->n_total),
@@ -613,7 +619,7 @@ int upload_plan(mfd_handle* h) {
   size_t esz = h->fp32 ? sizeof(float) : sizeof(double);
   CK(cudaMalloc(&h->d_panel, std::max<int64_t>(h->panel_elems, 1) * esz));
   CK(cudaMalloc(&h->d_upool, std::max<int64_t>(h->upool_elems, 1) * esz));
-  CK(cudaMalloc(&h->d_diag, (size_t)std::max(1, h->max_large_count) * kFactB * kFactB * esz));
+  CK(cudaMalloc(&h->d_diag, (size_t)std::max<int64_t>(h->dinv_elems, 1) * esz));
   CK(h->d_a.alloc(h->nnz_total));
   CK(h->d_norms.alloc(8));
   return MFD_OK;
@@ -779,6 +785,7 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
   T* X = static_cast<T*>(h->d_X);
   T* V = static_cast<T*>(h->d_V);
   T* S = static_cast<T*>(h->d_S);
+  const T* dinv = static_cast<const T*>(h->d_diag);
   const int32_t* lists = h->d_lists.p;
   const int64_t ldx = h->n_total;
   const double w = sizeof(T);
@@ -806,8 +813,8 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       double fl = 0, by = 0;
       work(L.large, fl, by);
       record(h, st, MFD_K_SOLVE_LARGE, fl, by, [&] {
-        launch_fwd_large<T>(F, lists + L.large.off, L.large.count, L.large.param2, L.large_max_nf, panel, X, ldx, V,
-                            nrhs, st, &n);
+        launch_fwd_large<T>(F, lists + L.large.off, L.large.count, L.large.param2, L.large_max_nf, panel, dinv, X,
+                            ldx, V, nrhs, st, &n);
       });
     }
   }
@@ -817,8 +824,8 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       double fl = 0, by = 0;
       work(L.large, fl, by);
       record(h, st, MFD_K_SOLVE_LARGE, fl, by, [&] {
-        launch_bwd_large<T>(F, lists + L.large.off, L.large.count, L.large.param2, L.large_max_nf, panel, X, ldx, V,
-                            S, nrhs, st, &n);
+        launch_bwd_large<T>(F, lists + L.large.off, L.large.count, L.large.param2, L.large_max_nf, panel, dinv, X,
+                            ldx, V, S, nrhs, st, &n);
       });
     }
     for (const LaunchList& s : L.small) {

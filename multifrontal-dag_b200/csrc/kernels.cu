@@ -273,161 +273,240 @@ __global__ void __launch_bounds__(256) k_extend_add(DevFronts F, const int32_t* 
 //   k_trsm  : the rows below, X <- A L11^{-T} = A (L11^{-1})^T, a GEMM with K = w
 //   k_update: trailing C(lower) -= P P^T with P the solved panel rows
 
-// Diagonal-block POTRF + inverse, one CTA per front, w <= 128.  The lower
-// triangle is split into 4x4 tiles (528 for w = 128) and each of the 544
-// threads keeps one tile in registers.  Cholesky: at pivot k the owners of tile
-// column k/4 publish column k into a double-buffered shared array, one barrier,
-// then every thread applies A -= c_k c_k^T / d_k to its tile (unscaled columns;
-// L(:,k) = c_k / sqrt(d_k) at the end).  Inverse: forward substitution on the
-// identity in place, one barrier per row (row j and column j published, row j's
-// 1/L_jj scaling deferred to step j+1).  L11 goes to the panel, L11^{-1} to linv.
-constexpr int kPotrfThreads = 544;
+// Diagonal-block POTRF + inverse, one CTA (8 warps) per front, w <= 128, all
+// arithmetic in FP64 whatever the storage type (the FP32 path's diagonal
+// blocks are thus factored with the FP64 fallback always taken; the kernel is
+// latency bound, so FP64 costs nothing here).
+//
+// The block (zero-padded to wp = 32 * ceil(w / 32), identity on the padded
+// diagonal) sits in shared memory S, column-major, ld kPLd.  Right-looking
+// over 32-wide sub-blocks b:
+//   1. warp 0: Cholesky of the 32 x 32 diagonal sub-block, one row per lane,
+//      pivots by shuffle, 1/sqrt by rsqrt (no division), column broadcast
+//      through a double-buffered shared vector; then the sub-block's inverse
+//      D_b by forward substitution, one column per lane;
+//   2. sub-panel below: L_ib = A_ib D_b^T, one 32-row tile per warp (DMMA);
+//   3. trailing update S_ij -= L_ib L_jb^T, 32 x 32 lower tiles over the warps
+//      (DMMA).
+// Then the full inverse X = L^{-1}: X_bb = D_b and, per block row r,
+// X_rc = -D_r (sum_{k=c}^{r-1} L_rk X_kc), one warp per block column c; the
+// off-diagonal X blocks are kept transposed in the strict upper part of S.
+// L goes to the panel, X (column-major, ld 128, zero outside the lower w x w)
+// to linv.  A non-positive pivot records its 1-based column in info (atomic
+// min) and continues with pivot 1.
+constexpr int kPotrfThreads = 256;
+constexpr int kPSub = 32;
+constexpr int kPLd = kFactB + 4;   // 132: ld = 4 mod 16 doubles keeps DMMA fragment loads conflict-free
+constexpr int kDLd = kPSub + 4;    // 36
+constexpr size_t kPotrfSmem =
+    sizeof(double) * ((size_t)kFactB * kPLd + (size_t)(kFactB / kPSub) * kPSub * kDLd +
+                      (size_t)(kFactB / kPSub - 1) * kPSub * kDLd + kFactB + 2 * kPSub);
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// One warp: acc(32 x 32) += A(32 x K) B(K x 32), K a multiple of 4, operands
+// in shared memory addressed as A(i, k) = A[i * ai + k * ak] and
+// B(k, j) = B[k * bk + j * bj].  acc[m][n][e] holds C(8m + g, 8n + 2q + e)
+// with g = lane / 4, q = lane % 4 (the m8n8k4 accumulator layout).
+__device__ __forceinline__ void warp_mm32(double (&acc)[4][4][2], const double* A, int ai, int ak, const double* B,
+                                          int bk, int bj, int K, int lane) {
+  const int g = lane >> 2, q = lane & 3;
+  for (int k = 0; k < K; k += 4) {
+    double a[4], b[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) a[m] = A[(8 * m + g) * ai + (k + q) * ak];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) b[n] = B[(k + q) * bk + (8 * n + g) * bj];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int n = 0; n < 4; ++n) dmma(acc[m][n][0], acc[m][n][1], a[m], b[n]);
+  }
+}
+
+__device__ __forceinline__ void acc_zero(double (&acc)[4][4][2]) {
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int n = 0; n < 4; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
+}
+
+// store s * acc at C(i, j) = C[i * ci + j * cj]
+__device__ __forceinline__ void acc_store(const double (&acc)[4][4][2], double* C, int ci, int cj, double s,
+                                          int lane) {
+  const int g = lane >> 2, q = lane & 3;
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) C[(8 * m + g) * ci + (8 * n + 2 * q + e) * cj] = s * acc[m][n][e];
+}
+
+// warp 0 of the CTA: Cholesky of S(o:o+32, o:o+32) in place, rsqrt of the
+// pivots into rq[o..o+31], inverse of the factor into D (column-major, ld kDLd,
+// zero above the diagonal).  Returns the 1-based sub-block pivot that failed, or 0.
+__device__ int warp_chol32(double* S, int o, double* D, double* rq, double* cbuf, int lane) {
+  double a[kPSub];
+#pragma unroll
+  for (int j = 0; j < kPSub; ++j) a[j] = S[(o + lane) + (o + j) * kPLd];
+  int bad = 0;
+#pragma unroll
+  for (int k = 0; k < kPSub; ++k) {
+    double d = __shfl_sync(0xffffffffu, a[k], k);
+    if (!(d > 0.0)) {               // uniform: every lane holds the same d
+      if (!bad) bad = k + 1;
+      d = 1.0;
+    }
+    const double y = rsqrt(d);
+    const double l = a[k] * y;
+    double* cb = cbuf + (k & 1) * kPSub;
+    cb[lane] = l;
+    if (lane == 0) rq[o + k] = y;
+    __syncwarp();
+    a[k] = lane == k ? d * y : l;
+#pragma unroll
+    for (int j = k + 1; j < kPSub; ++j) a[j] = fma(-l, cb[j], a[j]);
+  }
+#pragma unroll
+  for (int j = 0; j < kPSub; ++j)
+    if (j <= lane) S[(o + lane) + (o + j) * kPLd] = a[j];
+  __syncwarp();
+  // inverse: lane j owns column j of X = L^{-1}; forward substitution on e_j
+  double x[kPSub];
+#pragma unroll
+  for (int i = 0; i < kPSub; ++i) x[i] = i == lane ? 1.0 : 0.0;
+#pragma unroll
+  for (int k = 0; k < kPSub; ++k) {
+    x[k] *= rq[o + k];
+#pragma unroll
+    for (int i = k + 1; i < kPSub; ++i) x[i] = fma(-S[(o + i) + (o + k) * kPLd], x[k], x[i]);
+  }
+#pragma unroll
+  for (int i = 0; i < kPSub; ++i) D[i + lane * kDLd] = x[i];
+  return bad;
+}
+
+// Inverted diagonal block of panel step `step` of front f: persistent per front
+// when the plan provides d_off (kept for the solves), else one slot per list
+// entry of the launch.
+template <typename T>
+__device__ __forceinline__ T* inv_block(const DevFronts& F, T* linv, int f, int step, int slot) {
+  return F.d_off ? linv + F.d_off[f] + (size_t)step * kFactB * kFactB : linv + (size_t)slot * kFactB * kFactB;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const int32_t* list, int step, T* panel,
                                                             T* linv, int32_t* info) {
   constexpr int B = kFactB;
-  __shared__ T colbuf[2][B];
-  __shared__ T rowbuf[2][B];
-  __shared__ T piv[B];
-  __shared__ T rs[B];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* S = reinterpret_cast<double*>(smem_raw);
+  double* Dv = S + (size_t)B * kPLd;                         // 4 blocks of kPSub x kDLd
+  double* Yv = Dv + (size_t)(B / kPSub) * kPSub * kDLd;       // 3 blocks
+  double* rq = Yv + (size_t)(B / kPSub - 1) * kPSub * kDLd;   // B
+  double* cbuf = rq + B;                                      // 2 x kPSub
   const int f = list[blockIdx.x];
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int c0 = step * B;
   if (c0 >= nc) return;
   const int w = min(B, nc - c0);
-  const int tid = threadIdx.x;
-  const int nt = (w + 3) / 4, ntiles = nt * (nt + 1) / 2;
+  const int nsb = (w + kPSub - 1) / kPSub, wp = nsb * kPSub;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   T* P = panel + F.panel_off[f];
-  const bool own = tid < ntiles;
-  int tr = 0, tc = 0;
-  if (own) {
-    tr = (int)((sqrtf(8.0f * (float)tid + 1.0f) - 1.0f) * 0.5f);
-    while ((tr + 1) * (tr + 2) / 2 <= tid) ++tr;
-    while (tr * (tr + 1) / 2 > tid) --tr;
-    tc = tid - tr * (tr + 1) / 2;
-  }
-  const int i0 = 4 * tr, j0 = 4 * tc;
-  T tl[4][4];
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int i = i0 + u, j = j0 + v;
-      tl[u][v] = (own && i < w && j <= i) ? P[(c0 + i) + (size_t)(c0 + j) * nf] : T(0);
+  // ---- load the lower w x w block, identity on the padding ----
+  for (int e = tid; e < wp * wp; e += kPotrfThreads) {
+    const int i = e % wp, j = e / wp;
+    double v = 0.0;
+    if (i < w && j < w) {
+      if (i >= j) v = (double)P[(c0 + i) + (size_t)(c0 + j) * nf];
+    } else if (i == j) {
+      v = 1.0;
     }
-  // ---- Cholesky, one barrier per pivot ----
-  for (int k = 0; k < w; ++k) {
-    T* cb = colbuf[k & 1];
-    if (own && tc == (k >> 2)) {
-      const int kv = k & 3;           // explicit select keeps the tile in registers
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = i0 + u;
-        const T val = kv == 0 ? tl[u][0] : (kv == 1 ? tl[u][1] : (kv == 2 ? tl[u][2] : tl[u][3]));
-        if (i >= k && i < w) cb[i] = val;
-      }
-    }
-    __syncthreads();
-    T d = cb[k];
-    if (!(d > T(0))) {
-      if (tid == 0) atomicMin(info, F.first[f] + c0 + k + 1);
-      d = T(1);
-    }
-    if (tid == 0) piv[k] = d;
-    if (own && i0 + 3 > k) {
-      const T inv = T(1) / d;
-      T ci[4], cj[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = i0 + u;
-        ci[u] = (i > k && i < w) ? cb[i] : T(0);
-      }
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int j = j0 + v;
-        cj[v] = (j > k && j < w) ? cb[j] * inv : T(0);
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v)
-          if (j0 + v <= i0 + u) tl[u][v] -= ci[u] * cj[v];
-    }
+    S[i + j * kPLd] = v;
   }
   __syncthreads();
-  for (int j = tid; j < w; j += blockDim.x) rs[j] = T(1) / dev_sqrt<T>(piv[j]);
-  __syncthreads();
-  if (own) {
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int i = i0 + u, j = j0 + v;
-        if (i < w && j <= i) {
-          const T l = i == j ? dev_sqrt<T>(piv[j]) : tl[u][v] * rs[j];
-          tl[u][v] = l;
-          P[(c0 + i) + (size_t)(c0 + j) * nf] = l;
-        }
-      }
-  }
-  // ---- in-place inverse, one barrier per row ----
-  for (int j = 0; j < w; ++j) {
-    T* rb = rowbuf[j & 1];
-    T* cb = colbuf[j & 1];
-    if (own) {
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-          const int i = i0 + u, jj = j0 + v;
-          if (i == j && jj < j) rb[jj] = tl[u][v];
-          if (jj == j && i > j && i < w) cb[i] = tl[u][v];
-        }
+  // ---- right-looking over 32-wide sub-blocks ----
+  for (int b = 0; b < nsb; ++b) {
+    const int o = b * kPSub;
+    double* Db = Dv + (size_t)b * kPSub * kDLd;
+    if (warp == 0) {
+      const int bad = warp_chol32(S, o, Db, rq, cbuf, lane);
+      if (bad && lane == 0 && o + bad <= w) atomicMin(info, F.first[f] + c0 + o + bad);
     }
     __syncthreads();
-    if (own && i0 + 3 >= j - 1 && j0 <= j) {
-      const T r = rs[j];
-      const T rp = j >= 1 ? rs[j - 1] : T(0);
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = i0 + u;
-        const T lik = (i > j && i < w) ? cb[i] * r : T(0);
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-          const int jp = j0 + v;
-          if (i > j && i < w && jp <= j) tl[u][v] = jp < j ? tl[u][v] - lik * rb[jp] : -lik;
-          if (j >= 1 && i == j - 1 && jp <= j - 1) tl[u][v] = jp == j - 1 ? rp : tl[u][v] * rp;
-        }
-      }
+    const int rt = nsb - b - 1;                 // 32-row tiles below the sub-block
+    if (rt == 0) break;
+    if (warp < rt) {                            // L_ib = A_ib D_b^T, in place
+      const int r0 = o + kPSub + warp * kPSub;
+      double acc[4][4][2];
+      acc_zero(acc);
+      warp_mm32(acc, S + r0 + o * kPLd, 1, kPLd, Db, kDLd, 1, kPSub, lane);
+      __syncwarp();
+      acc_store(acc, S + r0 + o * kPLd, 1, kPLd, 1.0, lane);
     }
-  }
-  if (own) {
-    const T rl = rs[w - 1];
+    __syncthreads();
+    for (int t = warp; t < rt * (rt + 1) / 2; t += kPotrfThreads / 32) {   // trailing lower tiles
+      int ti = 0;
+      while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+      const int tj = t - ti * (ti + 1) / 2;
+      const int r0 = o + kPSub + ti * kPSub, q0 = o + kPSub + tj * kPSub;
+      double acc[4][4][2];
+      acc_zero(acc);
+      warp_mm32(acc, S + r0 + o * kPLd, 1, kPLd, S + q0 + o * kPLd, kPLd, 1, kPSub, lane);
+      const int g = lane >> 2, q = lane & 3;
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+      for (int m = 0; m < 4; ++m)
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int i = i0 + u, jp = j0 + v;
-        if (i == w - 1 && jp <= w - 1) tl[u][v] = jp == w - 1 ? rl : tl[u][v] * rl;
-      }
+        for (int n = 0; n < 4; ++n)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) S[(r0 + 8 * m + g) + (q0 + 8 * n + 2 * q + e) * kPLd] -= acc[m][n][e];
+    }
+    __syncthreads();
   }
-  T* Li = linv + (size_t)blockIdx.x * B * B;          // column-major, ld = B, zero outside the lower w x w
-  for (int e = tid; e < B * B; e += blockDim.x) {
+  // ---- inverse: X_rc = -D_r sum_{k=c}^{r-1} L_rk X_kc, X_rc stored transposed at S(32c + j, 32r + i) ----
+  for (int r = 1; r < nsb; ++r) {
+    if (warp < r) {
+      const int c = warp;
+      double acc[4][4][2];
+      acc_zero(acc);
+      // k = c: X_cc = D_c, B(k', j) = D_c(k', j)
+      warp_mm32(acc, S + r * kPSub + c * kPSub * kPLd, 1, kPLd, Dv + (size_t)c * kPSub * kDLd, 1, kDLd, kPSub,
+                lane);
+      for (int k = c + 1; k < r; ++k)   // B(k', j) = X_kc(k', j) = S(32c + j, 32k + k')
+        warp_mm32(acc, S + r * kPSub + k * kPSub * kPLd, 1, kPLd, S + c * kPSub + k * kPSub * kPLd, kPLd, 1, kPSub,
+                  lane);
+      double* Y = Yv + (size_t)c * kPSub * kDLd;
+      acc_store(acc, Y, 1, kDLd, 1.0, lane);
+      __syncwarp();
+      acc_zero(acc);
+      warp_mm32(acc, Dv + (size_t)r * kPSub * kDLd, 1, kDLd, Y, 1, kDLd, kPSub, lane);
+      acc_store(acc, S + c * kPSub + r * kPSub * kPLd, kPLd, 1, -1.0, lane);   // transposed
+    }
+    __syncthreads();
+  }
+  // ---- write L11 to the panel and X to linv ----
+  for (int e = tid; e < w * w; e += kPotrfThreads) {
+    const int i = e % w, j = e / w;
+    if (i >= j) P[(c0 + i) + (size_t)(c0 + j) * nf] = (T)S[i + j * kPLd];
+  }
+  T* Li = inv_block(F, linv, f, step, blockIdx.x);
+  for (int e = tid; e < B * B; e += kPotrfThreads) {
     const int i = e % B, j = e / B;
-    if (!(i < w && j < w && i >= j)) Li[e] = T(0);
-  }
-  if (own) {
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int i = i0 + u, j = j0 + v;
-        if (i < w && j <= i) Li[i + j * B] = tl[u][v];
-      }
+    double v = 0.0;
+    if (i < w && j < w && i >= j) {
+      const int bi = i / kPSub, bj = j / kPSub;
+      v = bi == bj ? Dv[(size_t)bi * kPSub * kDLd + (i - bi * kPSub) + (j - bj * kPSub) * kDLd] : S[j + i * kPLd];
+    }
+    Li[e] = (T)v;
   }
 }
 
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc, bool valid) {
+
   unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
   int sz = valid ? 8 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(sz));
@@ -436,11 +515,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
 
 // TRSM on the FP64 tensor pipe: 64 rows x w columns of the panel per CTA,
 // X = A Li^T with Li = L11^{-1}; 8 warps as 2 (rows) x 4 (columns) of 32x32.
@@ -458,7 +532,7 @@ __global__ void __launch_bounds__(256, 1) k_trsm_dmma(DevFronts F, const int32_t
   const int r0 = c0 + w + blockIdx.x * kTrRows;
   if (r0 >= nf) return;
   double* P = panel + F.panel_off[f];
-  const double* Li = linv + (size_t)blockIdx.y * kFactB * kFactB;
+  const double* Li = inv_block(F, linv, f, step, blockIdx.y);
   const int wp = (w + 3) & ~3;
   for (int e = threadIdx.x; e < kTrRows * wp; e += blockDim.x) {
     int k = e / kTrRows, r = e - k * kTrRows;
@@ -516,7 +590,7 @@ __global__ void __launch_bounds__(256) k_trsm_simt(DevFronts F, const int32_t* l
   const int r0 = c0 + w + blockIdx.x * kTrRows;
   if (r0 >= nf) return;
   T* P = panel + F.panel_off[f];
-  const T* Li = linv + (size_t)blockIdx.y * kFactB * kFactB;
+  const T* Li = inv_block(F, linv, f, step, blockIdx.y);
   for (int e = threadIdx.x; e < kTrRows * w; e += blockDim.x) {
     int k = e / kTrRows, r = e - k * kTrRows;
     As[k * LDA + r] = (r0 + r < nf) ? P[(r0 + r) + (size_t)(c0 + k) * nf] : T(0);
@@ -813,6 +887,17 @@ __global__ void __launch_bounds__(256) k_bwd_small(DevFronts F, const int32_t* l
 }
 
 // ---- large fronts: the solve vector of front f lives in V (nf per RHS) --------
+// Panel steps of kSolveB = 128 columns use the inverted diagonal blocks kept
+// from the factorization (Li = L_ss^{-1}), so a step is two GEMV/GEMM-shaped
+// launches and no sequential column loop:
+//   forward : y_s = Li v_s (k_fwd_large_diag), v_rest -= L_rest,s y_s (k_fwd_large_rest)
+//   backward: t_s = v_s - L_rest,s^T x_rest (k_bwd_large_rest partial sums per
+//             256-row chunk, summed in chunk order: deterministic), x_s = Li^T t_s
+//             (k_bwd_large_diag)
+// The diag kernels write the front's own entries of X directly.
+constexpr int kRhsG = 8;      // right-hand sides per pass
+constexpr int kFwdRows = 32;  // rows per CTA of k_fwd_large_rest
+
 template <typename T>
 __global__ void k_fwd_large_gather(DevFronts F, const int32_t* list, const T* X, int64_t ldx, T* V, int nrhs) {
   const int f = list[blockIdx.x];
@@ -832,74 +917,108 @@ __global__ void k_fwd_large_gather(DevFronts F, const int32_t* list, const T* X,
   }
 }
 
-// diagonal block of panel `step`: y = L_ss^{-1} v_s (forward) in one CTA
+// y_s = Li v_s: thread (row i, half h) sums k in [64h, 64h + 64) for a group of
+// 8 right-hand sides (Li is zero above its diagonal and outside w x w, so the
+// loops have fixed trip counts and the loads pipeline); halves meet in shared memory
 template <typename T>
 __global__ void __launch_bounds__(256) k_fwd_large_diag(DevFronts F, const int32_t* list, int step,
-                                                        const T* __restrict__ panel, T* V, int nrhs) {
-  __shared__ T D[kSolveB * (kSolveB + 1)];
-  __shared__ T vs[kSolveB];
+                                                        const T* __restrict__ dinv, T* X, int64_t ldx, T* V,
+                                                        int nrhs) {
+  __shared__ T vs[kSolveB * kRhsG];
+  __shared__ T hs[kSolveB * kRhsG];
   const int f = list[blockIdx.x];
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int c0 = step * kSolveB;
   if (c0 >= nc) return;
   const int w = min(kSolveB, nc - c0);
-  const T* P = panel + F.panel_off[f];
-  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-    int j = e / w, i = e - j * w;
-    if (i >= j) D[i + j * (kSolveB + 1)] = P[(c0 + i) + (size_t)(c0 + j) * nf];
-  }
-  for (int r = 0; r < nrhs; ++r) {
-    T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
+  const T* Li = inv_block(F, dinv, f, step, blockIdx.x);
+  T* Vf = V + F.v_off[f] * nrhs;
+  const int first = F.first[f];
+  const int tid = threadIdx.x, i = tid & (kSolveB - 1), h = tid >> 7;
+  for (int r0 = 0; r0 < nrhs; r0 += kRhsG) {
+    const int g = min(kRhsG, nrhs - r0);
     __syncthreads();
-    for (int i = threadIdx.x; i < w; i += blockDim.x) vs[i] = Vf[c0 + i];
-    __syncthreads();
-    if (threadIdx.x < 32) {        // one warp: sequential columns, lanes over rows
-      for (int k = 0; k < w; ++k) {
-        T yk = vs[k] / D[k + k * (kSolveB + 1)];
-        __syncwarp();
-        for (int i = k + 1 + threadIdx.x; i < w; i += 32) vs[i] -= D[i + k * (kSolveB + 1)] * yk;
-        if (threadIdx.x == 0) vs[k] = yk;
-        __syncwarp();
-      }
+    for (int e = tid; e < kSolveB * kRhsG; e += blockDim.x) {
+      const int k = e % kSolveB, r = e / kSolveB;
+      vs[k * kRhsG + r] = (k < w && r < g) ? Vf[(int64_t)(r0 + r) * nf + c0 + k] : T(0);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < w; i += blockDim.x) Vf[c0 + i] = vs[i];
+    T acc[kRhsG];
+#pragma unroll
+    for (int u = 0; u < kRhsG; ++u) acc[u] = T(0);
+#pragma unroll 16
+    for (int kk = 0; kk < kSolveB / 2; ++kk) {
+      const int k = h * (kSolveB / 2) + kk;
+      const T l = Li[i + k * kSolveB];
+#pragma unroll
+      for (int u = 0; u < kRhsG; ++u) acc[u] += l * vs[k * kRhsG + u];
+    }
+    if (h == 1)
+#pragma unroll
+      for (int u = 0; u < kRhsG; ++u) hs[i * kRhsG + u] = acc[u];
+    __syncthreads();
+    if (h == 0 && i < w) {
+#pragma unroll
+      for (int u = 0; u < kRhsG; ++u) {
+        if (u < g) {
+          const T y = acc[u] + hs[i * kRhsG + u];
+          const int r = r0 + u;
+          Vf[(int64_t)r * nf + c0 + i] = y;
+          X[first + c0 + i + r * ldx] = y;
+        }
+      }
+    }
   }
 }
 
-// rows below the diagonal block: v_i -= sum_k L(i, c0+k) y_k
+// v_rest -= L_rest,s y_s: 32 rows per CTA (lane = row), warp q takes panel
+// columns 16q .. 16q+15 (held in registers), partial sums reduced in shared memory
 template <typename T>
-__global__ void __launch_bounds__(kSolveRows) k_fwd_large_gemv(DevFronts F, const int32_t* list, int step,
-                                                               const T* __restrict__ panel, T* V, int nrhs) {
-  __shared__ T ys[kSolveB];
+__global__ void __launch_bounds__(256) k_fwd_large_rest(DevFronts F, const int32_t* list, int step,
+                                                        const T* __restrict__ panel, T* V, int nrhs) {
+  __shared__ T part[8][kRhsG][32];
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int c0 = step * kSolveB;
   if (c0 >= nc) return;
   const int w = min(kSolveB, nc - c0);
-  const int i = c0 + w + blockIdx.x * blockDim.x + threadIdx.x;
-  if (c0 + w + blockIdx.x * blockDim.x >= nf) return;
+  const int rbase = c0 + w + blockIdx.x * kFwdRows;
+  if (rbase >= nf) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int i = rbase + lane;
+  const bool valid = i < nf;
   const T* P = panel + F.panel_off[f];
-  for (int r = 0; r < nrhs; ++r) {
-    T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
-    __syncthreads();
-    if (threadIdx.x < w) ys[threadIdx.x] = Vf[c0 + threadIdx.x];
-    __syncthreads();
-    if (i < nf) {
-      T s = T(0);
-      for (int k = 0; k < w; ++k) s += P[i + (size_t)(c0 + k) * nf] * ys[k];
-      Vf[i] -= s;
-    }
+  T* Vf = V + F.v_off[f] * nrhs;
+  T lr[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const int col = warp * 16 + k;
+    lr[k] = (valid && col < w) ? P[i + (size_t)(c0 + col) * nf] : T(0);
   }
-}
-
-template <typename T>
-__global__ void k_fwd_large_finish(DevFronts F, const int32_t* list, T* X, int64_t ldx, const T* V, int nrhs) {
-  const int f = list[blockIdx.x];
-  const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
-  for (int r = 0; r < nrhs; ++r) {
-    const T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
-    for (int i = threadIdx.x; i < nc; i += blockDim.x) X[first + i + r * ldx] = Vf[i];
+  for (int r0 = 0; r0 < nrhs; r0 += kRhsG) {
+    const int g = min(kRhsG, nrhs - r0);
+#pragma unroll
+    for (int u = 0; u < kRhsG; ++u) {
+      T s = T(0);
+      if (u < g) {
+        const T* y = Vf + (int64_t)(r0 + u) * nf + c0 + warp * 16;
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+          if (warp * 16 + k < w) s += lr[k] * y[k];
+      }
+      part[warp][u][lane] = s;
+    }
+    __syncthreads();
+    {
+      const int u = threadIdx.x >> 5;
+      if (u < g && valid) {
+        T s = T(0);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) s += part[q][u][lane];
+        Vf[(int64_t)(r0 + u) * nf + i] -= s;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -914,80 +1033,125 @@ __global__ void k_bwd_large_gather(DevFronts F, const int32_t* list, const T* X,
   }
 }
 
-// partial sums of L(rows of this CTA, panel)^T v(rows): lanes over rows, warp reductions
+// partial sums of L_rest,s^T x_rest over one 256-row chunk: warp q takes rows
+// 32q .. 32q+31 of the chunk (lane = row, coalesced column reads),
+// 16 columns at a time for up to 4 right-hand sides, then a butterfly
+// transpose-reduce leaves column kb + (l mod 16)'s sum in lane l
+constexpr int kBwdG = 4;
 template <typename T>
-__global__ void __launch_bounds__(kSolveRows) k_bwd_large_gemvt(DevFronts F, const int32_t* list, int step,
-                                                                const T* __restrict__ panel, const T* V, T* scratch,
-                                                                int nrhs) {
-  __shared__ T part[kSolveRows / 32][kSolveB];
+__global__ void __launch_bounds__(256) k_bwd_large_rest(DevFronts F, const int32_t* list, int step,
+                                                        const T* __restrict__ panel, const T* V, T* scratch,
+                                                        int nrhs) {
+  __shared__ T part[8][kBwdG][kSolveB];
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int c0 = step * kSolveB;
   if (c0 >= nc) return;
   const int w = min(kSolveB, nc - c0);
-  const int rstart = c0 + w + blockIdx.x * blockDim.x;
-  const int nchunks = (nf - c0 - w + kSolveRows - 1) / kSolveRows;
-  if (rstart >= nf) return;
-  const int i = rstart + threadIdx.x;
+  const int rs0 = c0 + w;
+  const int rbase = rs0 + blockIdx.x * kSolveRows;
+  if (rbase >= nf) return;
+  const int nchunks = (nf - rs0 + kSolveRows - 1) / kSolveRows;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int i = rbase + warp * 32 + lane;
+  const bool valid = i < nf;
   const T* P = panel + F.panel_off[f];
-  for (int r = 0; r < nrhs; ++r) {
-    const T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
-    const T vi = i < nf ? Vf[i] : T(0);
-    for (int k = 0; k < w; ++k) {
-      T s = i < nf ? P[i + (size_t)(c0 + k) * nf] * vi : T(0);
+  const T* Vf = V + F.v_off[f] * nrhs;
+  for (int r0 = 0; r0 < nrhs; r0 += kBwdG) {
+    const int g = min(kBwdG, nrhs - r0);
+    T xi[kBwdG];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) part[warp][k] = s;
+    for (int u = 0; u < kBwdG; ++u) xi[u] = (valid && u < g) ? Vf[(int64_t)(r0 + u) * nf + i] : T(0);
+#pragma unroll 1
+    for (int kb = 0; kb < kSolveB; kb += 16) {
+      T pv[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) pv[j] = (valid && kb + j < w) ? P[i + (size_t)(c0 + kb + j) * nf] : T(0);
+#pragma unroll
+      for (int u = 0; u < kBwdG; ++u) {
+        if (u >= g) break;
+        T v[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = pv[j] * xi[u];
+#pragma unroll
+        for (int s = 8; s >= 1; s >>= 1) {
+          const bool up = (lane & s) != 0;
+#pragma unroll
+          for (int j = 0; j < s; ++j) {
+            const T send = up ? v[j] : v[j + s];
+            const T keep = up ? v[j + s] : v[j];
+            v[j] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+          }
+        }
+        v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);   // lanes l and l + 16 hold column kb + (l & 15)
+        if (lane < 16) part[warp][u][kb + lane] = v[0];
+      }
     }
     __syncthreads();
-    if (threadIdx.x < w) {
+    for (int e = threadIdx.x; e < g * kSolveB; e += blockDim.x) {
+      const int u = e / kSolveB, k = e % kSolveB;
       T s = T(0);
-      for (int q = 0; q < kSolveRows / 32; ++q) s += part[q][threadIdx.x];
-      scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + blockIdx.x) * kSolveB + threadIdx.x] = s;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) s += part[q][u][k];
+      scratch[F.s_off[f] * nrhs + ((int64_t)(r0 + u) * nchunks + blockIdx.x) * kSolveB + k] = s;
     }
     __syncthreads();
   }
 }
 
-// diagonal block (backward): t = v_s - sum of partial sums; L_ss^T y = t
+// t_s = v_s - sum over chunks; x_s = Li^T t_s: column i of Li is read by one
+// warp (lanes over k, coalesced; the warp's 16 columns loaded once) and reduced
+// with shuffles
 template <typename T>
 __global__ void __launch_bounds__(256) k_bwd_large_diag(DevFronts F, const int32_t* list, int step,
-                                                        const T* __restrict__ panel, T* V, const T* scratch,
-                                                        int nrhs) {
-  __shared__ T D[kSolveB * (kSolveB + 1)];
+                                                        const T* __restrict__ dinv, T* X, int64_t ldx, T* V,
+                                                        const T* scratch, int nrhs) {
+  constexpr int CW = kSolveB / 8;   // columns per warp
   __shared__ T ts[kSolveB];
   const int f = list[blockIdx.x];
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int c0 = step * kSolveB;
   if (c0 >= nc) return;
   const int w = min(kSolveB, nc - c0);
-  const int nchunks = (nf - c0 - w + kSolveRows - 1) / kSolveRows;
-  const T* P = panel + F.panel_off[f];
-  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-    int j = e / w, i = e - j * w;
-    if (i >= j) D[i + j * (kSolveB + 1)] = P[(c0 + i) + (size_t)(c0 + j) * nf];
-  }
+  const int rs0 = c0 + w;
+  const int nchunks = nf > rs0 ? (nf - rs0 + kSolveRows - 1) / kSolveRows : 0;
+  const T* Li = inv_block(F, dinv, f, step, blockIdx.x);
+  T* Vf = V + F.v_off[f] * nrhs;
+  const int first = F.first[f];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T lc[CW][kSolveB / 32];           // Li(lane + 32q, warp*CW + cc); zero above the diagonal
+#pragma unroll
+  for (int cc = 0; cc < CW; ++cc)
+#pragma unroll
+    for (int q = 0; q < kSolveB / 32; ++q) lc[cc][q] = Li[(lane + 32 * q) + (warp * CW + cc) * kSolveB];
   for (int r = 0; r < nrhs; ++r) {
-    T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
     __syncthreads();
-    for (int k = threadIdx.x; k < w; k += blockDim.x) {
-      T s = Vf[c0 + k];
-      for (int q = 0; q < nchunks; ++q) s -= scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + q) * kSolveB + k];
-      ts[k] = s;
+    if (threadIdx.x < kSolveB) {
+      T s = T(0);
+      if (threadIdx.x < w) {
+        s = Vf[(int64_t)r * nf + c0 + threadIdx.x];
+        for (int q = 0; q < nchunks; ++q)
+          s -= scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + q) * kSolveB + threadIdx.x];
+      }
+      ts[threadIdx.x] = s;
     }
     __syncthreads();
-    if (threadIdx.x < 32) {
-      for (int k = w - 1; k >= 0; --k) {
-        T yk = ts[k] / D[k + k * (kSolveB + 1)];
-        __syncwarp();
-        for (int m = threadIdx.x; m < k; m += 32) ts[m] -= D[k + m * (kSolveB + 1)] * yk;
-        if (threadIdx.x == 0) ts[k] = yk;
-        __syncwarp();
+    T tv[kSolveB / 32];
+#pragma unroll
+    for (int q = 0; q < kSolveB / 32; ++q) tv[q] = ts[lane + 32 * q];
+#pragma unroll
+    for (int cc = 0; cc < CW; ++cc) {
+      T s = T(0);
+#pragma unroll
+      for (int q = 0; q < kSolveB / 32; ++q) s += lc[cc][q] * tv[q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      const int i = warp * CW + cc;
+      if (lane == 0 && i < w) {
+        Vf[(int64_t)r * nf + c0 + i] = s;
+        X[first + c0 + i + r * ldx] = s;
       }
     }
-    __syncthreads();
-    for (int k = threadIdx.x; k < w; k += blockDim.x) Vf[c0 + k] = ts[k];
   }
 }
 
@@ -1097,6 +1261,7 @@ cudaError_t prepare_kernels() {
   chk(opt_in(k_small_front<double>)); chk(opt_in(k_small_front<float>));
   chk(opt_in(k_trsm_dmma)); chk(opt_in(k_trsm_simt<double>)); chk(opt_in(k_trsm_simt<float>));
   chk(opt_in(k_update_dmma));
+  chk(opt_in(k_potrf<double>)); chk(opt_in(k_potrf<float>));
   chk(opt_in(k_update_simt<double>)); chk(opt_in(k_update_simt<float>));
   chk(opt_in(k_fwd_small<double>)); chk(opt_in(k_fwd_small<float>));
   chk(opt_in(k_bwd_small<double>)); chk(opt_in(k_bwd_small<float>));
@@ -1157,7 +1322,7 @@ template <typename T>
 void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
                   cudaStream_t st) {
   if (count <= 0) return;
-  k_potrf<T><<<count, kPotrfThreads, 0, st>>>(F, list, step, panel, linv, info);
+  k_potrf<T><<<count, kPotrfThreads, kPotrfSmem, st>>>(F, list, step, panel, linv, info);
 }
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
@@ -1211,31 +1376,30 @@ void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf
 }
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
-                      T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st, int64_t* launches) {
+                      const T* dinv, T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st, int64_t* launches) {
   if (count <= 0) return;
   k_fwd_large_gather<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
-  int steps = ceil_div(max_nc, kSolveB);
-  int chunks = std::max(1, ceil_div(max_nf, kSolveRows));
+  const int steps = ceil_div(max_nc, kSolveB);
+  const int chunks = std::max(1, ceil_div(max_nf, kFwdRows));
   for (int s = 0; s < steps; ++s) {
-    k_fwd_large_diag<T><<<count, 256, 0, st>>>(F, list, s, panel, V, nrhs);
-    k_fwd_large_gemv<T><<<dim3(chunks, count), kSolveRows, 0, st>>>(F, list, s, panel, V, nrhs);
+    k_fwd_large_diag<T><<<count, 256, 0, st>>>(F, list, s, dinv, X, ldx, V, nrhs);
+    k_fwd_large_rest<T><<<dim3(chunks, count), 256, 0, st>>>(F, list, s, panel, V, nrhs);
   }
-  k_fwd_large_finish<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
-  if (launches) *launches += 2 + 2 * steps;
+  if (launches) *launches += 1 + 2 * steps;
 }
 template <typename T>
 void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
-                      T* X, int64_t ldx, T* V, T* scratch, int nrhs, cudaStream_t st, int64_t* launches) {
+                      const T* dinv, T* X, int64_t ldx, T* V, T* scratch, int nrhs, cudaStream_t st,
+                      int64_t* launches) {
   if (count <= 0) return;
   k_bwd_large_gather<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
-  int steps = ceil_div(max_nc, kSolveB);
-  int chunks = std::max(1, ceil_div(max_nf, kSolveRows));
+  const int steps = ceil_div(max_nc, kSolveB);
+  const int chunks = std::max(1, ceil_div(max_nf, kSolveRows));
   for (int s = steps - 1; s >= 0; --s) {
-    k_bwd_large_gemvt<T><<<dim3(chunks, count), kSolveRows, 0, st>>>(F, list, s, panel, V, scratch, nrhs);
-    k_bwd_large_diag<T><<<count, 256, 0, st>>>(F, list, s, panel, V, scratch, nrhs);
+    k_bwd_large_rest<T><<<dim3(chunks, count), 256, 0, st>>>(F, list, s, panel, V, scratch, nrhs);
+    k_bwd_large_diag<T><<<count, 256, 0, st>>>(F, list, s, dinv, X, ldx, V, scratch, nrhs);
   }
-  k_fwd_large_finish<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
-  if (launches) *launches += 2 + 2 * steps;
+  if (launches) *launches += 1 + 2 * steps;
 }
 
 template <typename T>
@@ -1289,10 +1453,10 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
                                     cudaStream_t);                                                                 \
   template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, int,         \
                                     cudaStream_t);                                                                 \
-  template void launch_fwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, T*, int64_t, T*,     \
-                                    int, cudaStream_t, int64_t*);                                                  \
-  template void launch_bwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, T*, int64_t, T*, T*, \
-                                    int, cudaStream_t, int64_t*);                                                  \
+  template void launch_fwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
+                                    int64_t, T*, int, cudaStream_t, int64_t*);                                     \
+  template void launch_bwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
+                                    int64_t, T*, T*, int, cudaStream_t, int64_t*);                                 \
   template void launch_permute_in<T>(const double*, int64_t, const int32_t*, T*, int64_t, int64_t, int,            \
                                      cudaStream_t);                                                                \
   template void launch_permute_out<T>(const T*, int64_t, const int32_t*, double*, int64_t, int64_t, int,           \

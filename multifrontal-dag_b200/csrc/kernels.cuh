@@ -14,8 +14,8 @@ constexpr int kFactB = 128;          // column panel of the blocked large-front 
 constexpr int kTrRowsH = 64;         // rows per CTA of the panel TRSM
 constexpr int kUpdTile = 128;        // trailing-update output tile (tensor path)
 constexpr int kUpdTileSimt = 64;     // trailing-update output tile (FMA path)
-constexpr int kSolveB = 64;          // column step of the large-front solves
-constexpr int kSolveRows = 256;      // rows per CTA in the large-front solve GEMV kernels
+constexpr int kSolveB = kFactB;      // column step of the large-front solves (one inverted diagonal block)
+constexpr int kSolveRows = 256;      // rows per CTA of the backward large-front partial sums
 
 // Opt every shared-memory-heavy kernel into the large dynamic shared memory
 // carve-out; called once per process before any launch or capture.
@@ -45,7 +45,8 @@ template <typename T>
 void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int max_nr, T* panel, T* upool,
                        cudaStream_t st);
 // Panel step s of the blocked large-front factorization (columns s*kFactB ..):
-//   potrf  : one CTA per front; L11 into the panel, L11^{-1} into linv (count x 128 x 128)
+//   potrf  : one CTA per front; L11 into the panel, L11^{-1} into linv (at DevFronts::d_off, or
+//            one 128 x 128 slot per list entry when d_off is null)
 //   trsm   : rows below the diagonal block, X <- X L11^{-T}   (kind 0: DMMA, 1: FMA)
 //   update : trailing lower triangle -= P P^T                  (kind 0: DMMA 128-tiles, 1: FMA 64-tiles)
 template <typename T>
@@ -65,12 +66,14 @@ void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf
 template <typename T>
 void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
                       int64_t ldx, int nrhs, cudaStream_t st);
+// Large fronts: dinv holds the inverted 128 x 128 diagonal blocks the factorization kept (DevFronts::d_off).
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
-                      T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st, int64_t* launches);
+                      const T* dinv, T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st, int64_t* launches);
 template <typename T>
 void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
-                      T* X, int64_t ldx, T* V, T* scratch, int nrhs, cudaStream_t st, int64_t* launches);
+                      const T* dinv, T* X, int64_t ldx, T* V, T* scratch, int nrhs, cudaStream_t st,
+                      int64_t* launches);
 
 // ---- vectors, residuals ---------------------------------------------------------
 template <typename T>

@@ -33,11 +33,13 @@ struct DevFronts {
   const int32_t* a_pos;       // per A entry: row + col*nf inside the front
   const int64_t* v_off;       // offset of f's solve vector (units of one RHS)
   const int64_t* s_off;       // scratch offset (large-front solve partial sums)
+  const int64_t* d_off;       // offset of f's inverted 128 x 128 diagonal blocks (one per panel step);
+                              // null: the inverse of list slot i lives at linv + i * 128 * 128
 };
 
 struct HostFront {
   int32_t nc, nr, first, parent, level, sys, node;
-  int64_t panel_off, u_off, v_off, s_off;
+  int64_t panel_off, u_off, v_off, s_off, d_off;
 };
 
 struct LaunchList {          // a list of front ids in the device list pool

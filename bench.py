@@ -40,6 +40,8 @@ WORKLOADS = {
                            make=lambda: P.laplace3d(64, 1), precision=1, max_zero=1000),
     "lap3d40": dict(desc="3D 7-point Laplacian 40^3 (n=64,000), small case for profiling captures",
                     make=lambda: P.laplace3d(40, 1), precision=0, max_zero=1000),
+    "lap3d40_fp32ir": dict(desc="3D 7-point Laplacian 40^3 (n=64,000), FP32 factor + FP64 refinement, small case for profiling",
+                           make=lambda: P.laplace3d(40, 1), precision=1, max_zero=1000),
     "lap2d100": dict(desc="2D 5-point Laplacian 100x100 (n=10,000), x* ~ U[-1,1] seed 0",
                      make=lambda: P.laplace2d(100, 0), precision=0, max_zero=10),
     "diff3d80": dict(desc="3D variable-coefficient diffusion 80^3 (n=512,000), FP32 factor + FP64 refinement",

@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "mfdag", "libmfdag.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["analysis.cpp", "kernels.cu", "api.cu", "noalloc.cu"]
+SOURCES = ["analysis.cpp", "kernels.cu", "update_tc.cu", "api.cu", "noalloc.cu"]
 
 
 def build(debug: bool = False, verbose: bool = False) -> str:

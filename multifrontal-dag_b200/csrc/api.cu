@@ -144,6 +144,8 @@ struct mfd_handle {
   int device = 0;
   mfd_options opt{};
   cudaStream_t st = nullptr;
+  cudaStream_t st2 = nullptr;                       // lookahead: trailing updates off the panel critical path
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   // systems
@@ -212,6 +214,9 @@ struct mfd_handle {
       if (p) cudaFree(p);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (st2) cudaStreamDestroy(st2);
     if (st) cudaStreamDestroy(st);
   }
 };
@@ -463,7 +468,7 @@ int upload_plan(mfd_handle* h) {
   CK(h->d_a_src.alloc(h->nnz_total));
   CK(h->d_a_pos.alloc(h->nnz_total));
   CK(h->d_sidx.alloc(h->nnz_total));
-  CK(h->d_info.alloc(1));
+  CK(h->d_info.alloc(2));   // [0] first bad pivot column, [1] bounded-wait expiry flag
   DevFronts& F = h->F;
   F.nc = h->d_nc.p; F.nr = h->d_nr.p; F.first = h->d_first.p; F.parent = h->d_parent.p;
   F.child_ptr = h->d_child_ptr.p; F.child = h->d_child.p; F.panel_off = h->d_panel_off.p; F.u_off = h->d_u_off.p;
@@ -620,6 +625,8 @@ int upload_plan(mfd_handle* h) {
   CK(cudaMalloc(&h->d_panel, std::max<int64_t>(h->panel_elems, 1) * esz));
   CK(cudaMalloc(&h->d_upool, std::max<int64_t>(h->upool_elems, 1) * esz));
   CK(cudaMalloc(&h->d_diag, (size_t)std::max<int64_t>(h->dinv_elems, 1) * esz));
+  // the inverted diagonal blocks are written on their lower w x w part only: the rest stays zero
+  CK(cudaMemsetAsync(h->d_diag, 0, (size_t)std::max<int64_t>(h->dinv_elems, 1) * esz, h->st));
   CK(h->d_a.alloc(h->nnz_total));
   CK(h->d_norms.alloc(8));
   return MFD_OK;
@@ -707,8 +714,10 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
   const bool prof = h->profiling;
   const int32_t* hl = h->h_lists.data();
   launch_fill_int(h->d_info.p, INT_MAX, 1, st);
-  ++n;
-  const int kind = h->opt.reserved[0] == 1 ? 1 : 0;   // 0: DMMA trailing update (FP64), 1: FFMA tiles
+  launch_fill_int(h->d_info.p + 1, 0, 1, st);
+  n += 2;
+  // trailing update: 0 tensor cores (FP64: DMMA; FP32: tcgen05 3xTF32), 1 FFMA tiles, 2 tcgen05 1xTF32 (FP32)
+  const int kind = h->opt.reserved[0];
   for (const LevelPlan& L : h->levels) {
     for (const LaunchList& s : L.small) {
       double fl = 0, by = 0;
@@ -743,9 +752,16 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
              [&] { launch_extend_add<T>(F, lists + e.off, e.count, e.param, panel, upool, st); });
       ++n;
     }
+    // Lookahead (on unless reserved[1] = 1; profiling runs the serial schedule so
+    // that every kernel is timed alone): after the TRSM of step s, the
+    // update tiles of the next panel's columns run on the main stream and the
+    // rest of the trailing update on the side stream, so POTRF/TRSM of step
+    // s+1 overlap it; the next step's update waits for it (shared columns).
+    const bool lookahead = h->opt.reserved[1] != 1 && !h->profiling;
+    bool pending = false;
     for (size_t s = 0; s < L.steps.size(); ++s) {
       const LaunchList& p = L.steps[s];
-      double pf = 0, pb = 0, tf = 0, tb = 0, uf = 0, ub = 0;
+      double pf = 0, pb = 0, tf = 0, tb = 0, uf = 0, ub = 0, uf1 = 0, ub1 = 0;
       if (prof)
         for (int i = 0; i < p.count; ++i) {
           const HostFront& f = h->fronts[hl[p.off + i]];
@@ -757,16 +773,42 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
           tb += w * (2.0 * nrem * wd + wd * wd);
           uf += 2.0 * wd * nrem * (nrem + 1) / 2;
           ub += w * (2.0 * nrem * (nrem + 1) / 2 + 2.0 * nrem * wd);
+          double n1 = std::min<double>(nrem, kFactB);          // next-panel columns
+          uf1 += 2.0 * wd * (n1 * (n1 + 1) / 2 + (nrem - n1) * n1);
+          ub1 += w * (2.0 * (n1 * (n1 + 1) / 2 + (nrem - n1) * n1) + 2.0 * nrem * wd);
         }
       record(h, st, MFD_K_PANEL, pf, pb,
              [&] { launch_potrf<T>(F, lists + p.off, p.count, (int)s, panel, diag, h->d_info.p, st); });
       record(h, st, MFD_K_TRSM, tf, tb,
-             [&] { launch_trsm<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, kind, st); });
-      record(h, st, MFD_K_UPDATE, uf, ub, [&] {
-        launch_update<T>(F, lists + p.off, p.count, (int)s, p.param2, p.param3, panel, upool, kind, st);
-      });
-      n += 3;
+             [&] { launch_trsm<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, kind == 1 ? 1 : 0, st); });
+      n += 2;
+      auto update = [&](cudaStream_t us, int mode) {
+        if constexpr (sizeof(T) == 4) {
+          if (kind == 0 || kind == 2) {
+            launch_update_tc(F, lists + p.off, p.count, (int)s, p.param2, reinterpret_cast<float*>(panel),
+                             reinterpret_cast<float*>(upool), kind == 0 ? 1 : 0, h->d_info.p + 1, us, mode);
+            return;
+          }
+        }
+        launch_update<T>(F, lists + p.off, p.count, (int)s, p.param2, p.param3, panel, upool, kind == 1 ? 1 : 0, us,
+                         mode);
+      };
+      if (pending) cudaStreamWaitEvent(st, h->ev_join, 0);
+      pending = false;
+      if (lookahead && s + 1 < L.steps.size()) {
+        cudaEventRecord(h->ev_fork, st);
+        cudaStreamWaitEvent(h->st2, h->ev_fork, 0);
+        record(h, h->st2, MFD_K_UPDATE, uf - uf1, ub - ub1, [&] { update(h->st2, 2); });
+        record(h, st, MFD_K_UPDATE, uf1, ub1, [&] { update(st, 1); });
+        cudaEventRecord(h->ev_join, h->st2);
+        pending = true;
+        n += 2;
+      } else {
+        record(h, st, MFD_K_UPDATE, uf, ub, [&] { update(st, 0); });
+        ++n;
+      }
     }
+    if (pending) cudaStreamWaitEvent(st, h->ev_join, 0);
   }
   // values of the permuted full matrix for residuals
   record(h, st, MFD_K_OTHER, 0, 0, [&] {
@@ -852,7 +894,9 @@ int run_graph(mfd_handle* h, cudaGraphExec_t* exec, Fn&& fn) {
     fn(h->st);
     cudaError_t e = cudaStreamEndCapture(h->st, &g);
     if (e != cudaSuccess) return fail(MFD_E_CUDA, std::string("capture: ") + cudaGetErrorString(e));
-    e = cudaGraphInstantiate(exec, g, 0);
+    // per-node priorities (captured from the streams): the panel chain of the
+    // lookahead outranks the side-stream trailing updates
+    e = cudaGraphInstantiateWithFlags(exec, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(MFD_E_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
   }
@@ -879,9 +923,9 @@ int do_factorize(mfd_handle* h, const double* a) {
                    : run_graph(h, &h->g_factor, [&](cudaStream_t s) { h->launches_factor = enqueue_factor<double>(h, s); });
   if (rc) return rc;
   CK(cudaEventRecord(h->ev1, h->st));
-  int32_t info = 0;
+  int32_t infos[2] = {0, 0};
   double anorm = 0;
-  CK(cudaMemcpyAsync(&info, h->d_info.p, sizeof(int32_t), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaMemcpyAsync(infos, h->d_info.p, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, h->st));
   CK(cudaMemcpyAsync(&anorm, h->d_norms.p + 7, sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   float ms = 0;
@@ -891,6 +935,11 @@ int do_factorize(mfd_handle* h, const double* a) {
   h->anorm = anorm;
   h->time_info[6] = ms * 1e-3;
   h->factored = true;
+  const int32_t info = infos[0];
+  if (infos[1] != 0) {
+    h->factored = false;
+    return fail(MFD_E_TIMEOUT, "a bounded wait in the tensor-core update expired");
+  }
   if (info != INT_MAX) {
     // map the global permuted column to the system-relative 1-based column
     int64_t col = info - 1;
@@ -1018,7 +1067,12 @@ int create_common(mfd_handle** out, std::vector<Symbolic>&& syms, const mfd_opti
   h->sys = std::move(syms);
   CK(cudaSetDevice(h->device));
   CK(prepare_kernels());
-  CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  int prio_lo = 0, prio_hi = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+  CK(cudaStreamCreateWithPriority(&h->st, cudaStreamNonBlocking, prio_hi));
+  CK(cudaStreamCreateWithPriority(&h->st2, cudaStreamNonBlocking, prio_lo));
+  CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
   CK(cudaEventCreate(&h->ev0));
   CK(cudaEventCreate(&h->ev1));
   int rc = build_plan(h.get());

@@ -38,6 +38,28 @@ template <>
 __device__ __forceinline__ float dev_sqrt<float>(float x) { return sqrtf(x); }
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// Strided element loop (e = threadIdx.x, += blockDim.x, e < total) whose
+// global loads are issued kBatch at a time before the matching stores, so a
+// thread keeps kBatch independent loads in flight instead of one.
+constexpr int kBatch = 16;
+template <typename Load, typename Store>
+__device__ __forceinline__ void batched_loop(int total, Load&& load, Store&& store) {
+  using V = decltype(load(0));
+  for (int e0 = threadIdx.x; e0 < total; e0 += blockDim.x * kBatch) {
+    V v[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int e = e0 + u * (int)blockDim.x;
+      v[u] = e < total ? load(e) : V(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int e = e0 + u * (int)blockDim.x;
+      if (e < total) store(e, v[u]);
+    }
+  }
+}
 inline int clamp_grid(int64_t g, int64_t cap = 65535) { return (int)std::max<int64_t>(1, std::min<int64_t>(g, cap)); }
 
 // ============================================================================
@@ -282,16 +304,19 @@ __global__ void __launch_bounds__(256) k_extend_add(DevFronts F, const int32_t* 
 // diagonal) sits in shared memory S, column-major, ld kPLd.  Right-looking
 // over 32-wide sub-blocks b:
 //   1. warp 0: Cholesky of the 32 x 32 diagonal sub-block, one row per lane,
-//      pivots by shuffle, 1/sqrt by rsqrt (no division), column broadcast
-//      through a double-buffered shared vector; then the sub-block's inverse
-//      D_b by forward substitution, one column per lane;
+//      pivots by shuffle, 1/sqrt by rsqrt (no division), the next column
+//      updated ahead of the rest (one shuffle) so the next pivot's 1/sqrt
+//      overlaps the rank-1 update, whose column broadcast goes through a
+//      double-buffered shared vector; then the sub-block's inverse D_b by
+//      forward substitution, one column per lane;
 //   2. sub-panel below: L_ib = A_ib D_b^T, one 32-row tile per warp (DMMA);
 //   3. trailing update S_ij -= L_ib L_jb^T, 32 x 32 lower tiles over the warps
 //      (DMMA).
 // Then the full inverse X = L^{-1}: X_bb = D_b and, per block row r,
-// X_rc = -D_r (sum_{k=c}^{r-1} L_rk X_kc), one warp per block column c; the
+// X_rc = -D_r (sum_{k=c}^{r-1} L_rk X_kc), two warps per block column c; the
 // off-diagonal X blocks are kept transposed in the strict upper part of S.
-// L goes to the panel, X (column-major, ld 128, zero outside the lower w x w)
+// L goes to the panel, X (column-major, ld 128, zero outside the lower w x w;
+// persistent blocks are zeroed at allocation and written on that part only)
 // to linv.  A non-positive pivot records its 1-based column in info (atomic
 // min) and continues with pivot 1.
 constexpr int kPotrfThreads = 256;
@@ -308,39 +333,42 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-// One warp: acc(32 x 32) += A(32 x K) B(K x 32), K a multiple of 4, operands
+// One warp: acc(8 MF x 32) += A(8 MF x K) B(K x 32), K a multiple of 4, operands
 // in shared memory addressed as A(i, k) = A[i * ai + k * ak] and
 // B(k, j) = B[k * bk + j * bj].  acc[m][n][e] holds C(8m + g, 8n + 2q + e)
 // with g = lane / 4, q = lane % 4 (the m8n8k4 accumulator layout).
-__device__ __forceinline__ void warp_mm32(double (&acc)[4][4][2], const double* A, int ai, int ak, const double* B,
+template <int MF>
+__device__ __forceinline__ void warp_mm32(double (&acc)[MF][4][2], const double* A, int ai, int ak, const double* B,
                                           int bk, int bj, int K, int lane) {
   const int g = lane >> 2, q = lane & 3;
   for (int k = 0; k < K; k += 4) {
-    double a[4], b[4];
+    double a[MF], b[4];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) a[m] = A[(8 * m + g) * ai + (k + q) * ak];
+    for (int m = 0; m < MF; ++m) a[m] = A[(8 * m + g) * ai + (k + q) * ak];
 #pragma unroll
     for (int n = 0; n < 4; ++n) b[n] = B[(k + q) * bk + (8 * n + g) * bj];
 #pragma unroll
-    for (int m = 0; m < 4; ++m)
+    for (int m = 0; m < MF; ++m)
 #pragma unroll
       for (int n = 0; n < 4; ++n) dmma(acc[m][n][0], acc[m][n][1], a[m], b[n]);
   }
 }
 
-__device__ __forceinline__ void acc_zero(double (&acc)[4][4][2]) {
+template <int MF>
+__device__ __forceinline__ void acc_zero(double (&acc)[MF][4][2]) {
 #pragma unroll
-  for (int m = 0; m < 4; ++m)
+  for (int m = 0; m < MF; ++m)
 #pragma unroll
     for (int n = 0; n < 4; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
 }
 
 // store s * acc at C(i, j) = C[i * ci + j * cj]
-__device__ __forceinline__ void acc_store(const double (&acc)[4][4][2], double* C, int ci, int cj, double s,
+template <int MF>
+__device__ __forceinline__ void acc_store(const double (&acc)[MF][4][2], double* C, int ci, int cj, double s,
                                           int lane) {
   const int g = lane >> 2, q = lane & 3;
 #pragma unroll
-  for (int m = 0; m < 4; ++m)
+  for (int m = 0; m < MF; ++m)
 #pragma unroll
     for (int n = 0; n < 4; ++n)
 #pragma unroll
@@ -355,22 +383,36 @@ __device__ int warp_chol32(double* S, int o, double* D, double* rq, double* cbuf
 #pragma unroll
   for (int j = 0; j < kPSub; ++j) a[j] = S[(o + lane) + (o + j) * kPLd];
   int bad = 0;
+  // pivot k's scale y and column l = L(lane, k) are formed one step ahead: at
+  // step k the next column is updated first (one shuffle), so pivot k+1's
+  // 1/sqrt overlaps the rest of step k's rank-1 update
+  double d = __shfl_sync(0xffffffffu, a[0], 0);
+  if (!(d > 0.0)) { bad = 1; d = 1.0; }
+  double y = rsqrt(d);
+  double l = a[0] * y;
 #pragma unroll
   for (int k = 0; k < kPSub; ++k) {
-    double d = __shfl_sync(0xffffffffu, a[k], k);
-    if (!(d > 0.0)) {               // uniform: every lane holds the same d
-      if (!bad) bad = k + 1;
-      d = 1.0;
-    }
-    const double y = rsqrt(d);
-    const double l = a[k] * y;
     double* cb = cbuf + (k & 1) * kPSub;
     cb[lane] = l;
     if (lane == 0) rq[o + k] = y;
-    __syncwarp();
     a[k] = lane == k ? d * y : l;
+    double dn = 1.0, yn = 1.0, ln = 0.0;
+    if (k + 1 < kPSub) {
+      a[k + 1] = fma(-l, __shfl_sync(0xffffffffu, l, k + 1), a[k + 1]);
+      dn = __shfl_sync(0xffffffffu, a[k + 1], k + 1);
+      if (!(dn > 0.0)) {               // uniform: every lane holds the same pivot
+        if (!bad) bad = k + 2;
+        dn = 1.0;
+      }
+      yn = rsqrt(dn);
+      ln = a[k + 1] * yn;
+    }
+    __syncwarp();
 #pragma unroll
-    for (int j = k + 1; j < kPSub; ++j) a[j] = fma(-l, cb[j], a[j]);
+    for (int j = k + 2; j < kPSub; ++j) a[j] = fma(-l, cb[j], a[j]);
+    d = dn;
+    y = yn;
+    l = ln;
   }
 #pragma unroll
   for (int j = 0; j < kPSub; ++j)
@@ -418,16 +460,22 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   T* P = panel + F.panel_off[f];
   // ---- load the lower w x w block, identity on the padding ----
-  for (int e = tid; e < wp * wp; e += kPotrfThreads) {
-    const int i = e % wp, j = e / wp;
-    double v = 0.0;
-    if (i < w && j < w) {
-      if (i >= j) v = (double)P[(c0 + i) + (size_t)(c0 + j) * nf];
-    } else if (i == j) {
-      v = 1.0;
-    }
-    S[i + j * kPLd] = v;
-  }
+  batched_loop(
+      B * B,
+      [&](int e) {
+        const int i = e % B, j = e / B;
+        double v = 0.0;
+        if (i < w && j < w) {
+          if (i >= j) v = (double)P[(c0 + i) + (size_t)(c0 + j) * nf];
+        } else if (i == j) {
+          v = 1.0;
+        }
+        return v;
+      },
+      [&](int e, double v) {
+        const int i = e % B, j = e / B;
+        if (i < wp && j < wp) S[i + j * kPLd] = v;
+      });
   __syncthreads();
   // ---- right-looking over 32-wide sub-blocks ----
   for (int b = 0; b < nsb; ++b) {
@@ -467,37 +515,45 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
     }
     __syncthreads();
   }
-  // ---- inverse: X_rc = -D_r sum_{k=c}^{r-1} L_rk X_kc, X_rc stored transposed at S(32c + j, 32r + i) ----
+  // ---- inverse: X_rc = -D_r sum_{k=c}^{r-1} L_rk X_kc, X_rc stored transposed at S(32c + j, 32r + i);
+  //      two warps per block column c, 16 rows each ----
   for (int r = 1; r < nsb; ++r) {
-    if (warp < r) {
-      const int c = warp;
-      double acc[4][4][2];
+    const int c = warp >> 1, h = warp & 1;
+    double* Y = Yv + (size_t)c * kPSub * kDLd;
+    if (c < r) {
+      double acc[2][4][2];
       acc_zero(acc);
       // k = c: X_cc = D_c, B(k', j) = D_c(k', j)
-      warp_mm32(acc, S + r * kPSub + c * kPSub * kPLd, 1, kPLd, Dv + (size_t)c * kPSub * kDLd, 1, kDLd, kPSub,
-                lane);
+      warp_mm32(acc, S + r * kPSub + 16 * h + c * kPSub * kPLd, 1, kPLd, Dv + (size_t)c * kPSub * kDLd, 1, kDLd,
+                kPSub, lane);
       for (int k = c + 1; k < r; ++k)   // B(k', j) = X_kc(k', j) = S(32c + j, 32k + k')
-        warp_mm32(acc, S + r * kPSub + k * kPSub * kPLd, 1, kPLd, S + c * kPSub + k * kPSub * kPLd, kPLd, 1, kPSub,
-                  lane);
-      double* Y = Yv + (size_t)c * kPSub * kDLd;
-      acc_store(acc, Y, 1, kDLd, 1.0, lane);
-      __syncwarp();
+        warp_mm32(acc, S + r * kPSub + 16 * h + k * kPSub * kPLd, 1, kPLd, S + c * kPSub + k * kPSub * kPLd, kPLd,
+                  1, kPSub, lane);
+      acc_store(acc, Y + 16 * h, 1, kDLd, 1.0, lane);
+    }
+    __syncthreads();
+    if (c < r) {
+      double acc[2][4][2];
       acc_zero(acc);
-      warp_mm32(acc, Dv + (size_t)r * kPSub * kDLd, 1, kDLd, Y, 1, kDLd, kPSub, lane);
-      acc_store(acc, S + c * kPSub + r * kPSub * kPLd, kPLd, 1, -1.0, lane);   // transposed
+      warp_mm32(acc, Dv + (size_t)r * kPSub * kDLd + 16 * h, 1, kDLd, Y, 1, kDLd, kPSub, lane);
+      acc_store(acc, S + c * kPSub + (r * kPSub + 16 * h) * kPLd, kPLd, 1, -1.0, lane);   // transposed
     }
     __syncthreads();
   }
   // ---- write L11 to the panel and X to linv ----
-  for (int e = tid; e < w * w; e += kPotrfThreads) {
-    const int i = e % w, j = e / w;
-    if (i >= j) P[(c0 + i) + (size_t)(c0 + j) * nf] = (T)S[i + j * kPLd];
-  }
-  T* Li = inv_block(F, linv, f, step, blockIdx.x);
   for (int e = tid; e < B * B; e += kPotrfThreads) {
     const int i = e % B, j = e / B;
+    if (i < w && j < w && i >= j) P[(c0 + i) + (size_t)(c0 + j) * nf] = (T)S[i + j * kPLd];
+  }
+  // persistent blocks (d_off) were zeroed once: only their lower w x w part is written
+  T* Li = inv_block(F, linv, f, step, blockIdx.x);
+  const bool full = F.d_off == nullptr;
+  for (int e = tid; e < B * B; e += kPotrfThreads) {
+    const int i = e % B, j = e / B;
+    const bool in = i < w && j < w && i >= j;
+    if (!in && !full) continue;
     double v = 0.0;
-    if (i < w && j < w && i >= j) {
+    if (in) {
       const int bi = i / kPSub, bj = j / kPSub;
       v = bi == bj ? Dv[(size_t)bi * kPSub * kDLd + (i - bi * kPSub) + (j - bj * kPSub) * kDLd] : S[j + i * kPLd];
     }
@@ -534,14 +590,16 @@ __global__ void __launch_bounds__(256, 1) k_trsm_dmma(DevFronts F, const int32_t
   double* P = panel + F.panel_off[f];
   const double* Li = inv_block(F, linv, f, step, blockIdx.y);
   const int wp = (w + 3) & ~3;
-  for (int e = threadIdx.x; e < kTrRows * wp; e += blockDim.x) {
-    int k = e / kTrRows, r = e - k * kTrRows;
-    As[k * kTrLdA + r] = (k < w && r0 + r < nf) ? P[(r0 + r) + (size_t)(c0 + k) * nf] : 0.0;
-  }
-  for (int e = threadIdx.x; e < kFactB * wp; e += blockDim.x) {
-    int k = e / kFactB, n = e - k * kFactB;
-    Bs[k * kTrLdB + n] = Li[n + k * kFactB];
-  }
+  batched_loop(
+      kTrRows * wp,
+      [&](int e) {
+        const int k = e / kTrRows, r = e - k * kTrRows;
+        return (k < w && r0 + r < nf) ? P[(r0 + r) + (size_t)(c0 + k) * nf] : 0.0;
+      },
+      [&](int e, double v) { As[(e / kTrRows) * kTrLdA + (e % kTrRows)] = v; });
+  batched_loop(
+      kFactB * wp, [&](int e) { return Li[(e % kFactB) + (e / kFactB) * kFactB]; },
+      [&](int e, double v) { Bs[(e / kFactB) * kTrLdB + (e % kFactB)] = v; });
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = warp >> 2, wn = warp & 3;
@@ -591,14 +649,16 @@ __global__ void __launch_bounds__(256) k_trsm_simt(DevFronts F, const int32_t* l
   if (r0 >= nf) return;
   T* P = panel + F.panel_off[f];
   const T* Li = inv_block(F, linv, f, step, blockIdx.y);
-  for (int e = threadIdx.x; e < kTrRows * w; e += blockDim.x) {
-    int k = e / kTrRows, r = e - k * kTrRows;
-    As[k * LDA + r] = (r0 + r < nf) ? P[(r0 + r) + (size_t)(c0 + k) * nf] : T(0);
-  }
-  for (int e = threadIdx.x; e < kFactB * w; e += blockDim.x) {
-    int k = e / kFactB, n = e - k * kFactB;
-    Bs[k * LDB + n] = Li[n + k * kFactB];
-  }
+  batched_loop(
+      kTrRows * w,
+      [&](int e) {
+        const int k = e / kTrRows, r = e - k * kTrRows;
+        return (r0 + r < nf) ? P[(r0 + r) + (size_t)(c0 + k) * nf] : T(0);
+      },
+      [&](int e, T v) { As[(e / kTrRows) * LDA + (e % kTrRows)] = v; });
+  batched_loop(
+      kFactB * w, [&](int e) { return Li[(e % kFactB) + (e / kFactB) * kFactB]; },
+      [&](int e, T v) { Bs[(e / kFactB) * LDB + (e % kFactB)] = v; });
   __syncthreads();
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   T acc[4][8];
@@ -626,13 +686,6 @@ __global__ void __launch_bounds__(256) k_trsm_simt(DevFronts F, const int32_t* l
     }
 }
 
-__device__ __forceinline__ void tile_of(int t, int& ti, int& tj) {
-  int i = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
-  while ((i + 1) * (i + 2) / 2 <= t) ++i;
-  while (i * (i + 1) / 2 > t) --i;
-  ti = i;
-  tj = t - i * (i + 1) / 2;
-}
 
 template <typename T>
 __device__ __forceinline__ T* trailing_addr(T* P, T* U, int nc, int nr, int nf, int gi, int gj) {
@@ -646,7 +699,7 @@ __device__ __forceinline__ T* trailing_addr(T* P, T* U, int nc, int nr, int nf, 
 // stride of 136 doubles, which makes the fragment loads conflict-free.
 constexpr int kUT = 128, kUK = 32, kULD = 136;
 __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32_t* list, int step, double* panel,
-                                                        double* upool) {
+                                                        double* upool, int mode) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* sm = reinterpret_cast<double*>(smem_raw);     // [stage][operand][k][row]
   const int f = list[blockIdx.y];
@@ -658,9 +711,8 @@ __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32
   const int nrem = nf - base;
   if (nrem <= 0) return;
   const int T = (nrem + kUT - 1) / kUT;
-  if ((int)blockIdx.x >= T * (T + 1) / 2) return;
   int ti, tj;
-  tile_of(blockIdx.x, ti, tj);
+  if (!select_tile(mode, T, kUT, blockIdx.x, ti, tj)) return;
   const int i0 = base + ti * kUT, j0 = base + tj * kUT;
   double* P = panel + F.panel_off[f];
   const int nchunks = (w + kUK - 1) / kUK;
@@ -747,7 +799,8 @@ __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32
 // 256 threads each 4x4 outputs (rows ty+16m, columns tx+16n).
 constexpr int kSimtTile = 64, kSimtK = 64;
 template <typename T>
-__global__ void __launch_bounds__(256) k_update_simt(DevFronts F, const int32_t* list, int step, T* panel, T* upool) {
+__global__ void __launch_bounds__(256) k_update_simt(DevFronts F, const int32_t* list, int step, T* panel, T* upool,
+                                                     int mode) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int LDK = kSimtTile + 4;
   T* As = reinterpret_cast<T*>(smem_raw);
@@ -761,9 +814,8 @@ __global__ void __launch_bounds__(256) k_update_simt(DevFronts F, const int32_t*
   const int nrem = nf - base;
   if (nrem <= 0) return;
   const int Tn = (nrem + kSimtTile - 1) / kSimtTile;
-  if ((int)blockIdx.x >= Tn * (Tn + 1) / 2) return;
   int ti, tj;
-  tile_of(blockIdx.x, ti, tj);
+  if (!select_tile(mode, Tn, kSimtTile, blockIdx.x, ti, tj)) return;
   const int i0 = base + ti * kSimtTile, j0 = base + tj * kSimtTile;
   T* P = panel + F.panel_off[f];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -775,12 +827,17 @@ __global__ void __launch_bounds__(256) k_update_simt(DevFronts F, const int32_t*
   for (int k0 = 0; k0 < w; k0 += kSimtK) {
     const int kw = min(kSimtK, w - k0);
     __syncthreads();
-    for (int e = threadIdx.x; e < kSimtTile * kw; e += blockDim.x) {
-      int k = e / kSimtTile, r = e - k * kSimtTile;
-      int gi = i0 + r, gj = j0 + r;
-      As[k * LDK + r] = gi < nf ? P[gi + (size_t)(c0 + k0 + k) * nf] : T(0);
-      Bs[k * LDK + r] = gj < nf ? P[gj + (size_t)(c0 + k0 + k) * nf] : T(0);
-    }
+    batched_loop(
+        2 * kSimtTile * kw,
+        [&](int e) {
+          const int op = e / (kSimtTile * kw), rem = e - op * (kSimtTile * kw);
+          const int k = rem / kSimtTile, g = (op ? j0 : i0) + rem % kSimtTile;
+          return g < nf ? P[g + (size_t)(c0 + k0 + k) * nf] : T(0);
+        },
+        [&](int e, T v) {
+          const int op = e / (kSimtTile * kw), rem = e - op * (kSimtTile * kw);
+          (op ? Bs : As)[(rem / kSimtTile) * LDK + rem % kSimtTile] = v;
+        });
     __syncthreads();
     for (int k = 0; k < kw; ++k) {
       T av[4], bv[4];
@@ -1262,6 +1319,7 @@ cudaError_t prepare_kernels() {
   chk(opt_in(k_trsm_dmma)); chk(opt_in(k_trsm_simt<double>)); chk(opt_in(k_trsm_simt<float>));
   chk(opt_in(k_update_dmma));
   chk(opt_in(k_potrf<double>)); chk(opt_in(k_potrf<float>));
+  chk(prepare_update_tc());
   chk(opt_in(k_update_simt<double>)); chk(opt_in(k_update_simt<float>));
   chk(opt_in(k_fwd_small<double>)); chk(opt_in(k_fwd_small<float>));
   chk(opt_in(k_bwd_small<double>)); chk(opt_in(k_bwd_small<float>));
@@ -1340,22 +1398,31 @@ void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, i
   size_t sm = ((size_t)kFactB * (kTrRows + 4) + (size_t)kFactB * (kFactB + 4)) * sizeof(T);
   k_trsm_simt<T><<<grid, 256, sm, st>>>(F, list, step, panel, linv);
 }
+int update_grid(int tiles, int tw, int mode) {
+  if (mode != 1) return tiles;
+  int T = 0;
+  while ((T + 1) * (T + 2) / 2 <= tiles) ++T;      // tiles = T (T + 1) / 2
+  return T * (kFactB / tw);
+}
+
 template <typename T>
 void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, int tiles64, T* panel,
-                   T* upool, int kind, cudaStream_t st) {
+                   T* upool, int kind, cudaStream_t st, int mode) {
   if (count <= 0) return;
   if constexpr (sizeof(T) == 8) {
     if (kind == 0) {
-      if (tiles128 <= 0) return;
+      const int g = update_grid(tiles128, kUT, mode);
+      if (g <= 0) return;
       size_t sm = 2 * 2 * (size_t)kUK * kULD * sizeof(double);
-      k_update_dmma<<<dim3(tiles128, count), 256, sm, st>>>(F, list, step, reinterpret_cast<double*>(panel),
-                                                              reinterpret_cast<double*>(upool));
+      k_update_dmma<<<dim3(g, count), 256, sm, st>>>(F, list, step, reinterpret_cast<double*>(panel),
+                                                      reinterpret_cast<double*>(upool), mode);
       return;
     }
   }
-  if (tiles64 <= 0) return;
+  const int g = update_grid(tiles64, kSimtTile, mode);
+  if (g <= 0) return;
   size_t sm = 2 * (size_t)kSimtK * (kSimtTile + 4) * sizeof(T);
-  k_update_simt<T><<<dim3(tiles64, count), 256, sm, st>>>(F, list, step, panel, upool);
+  k_update_simt<T><<<dim3(g, count), 256, sm, st>>>(F, list, step, panel, upool, mode);
 }
 
 template <typename T>
@@ -1448,7 +1515,8 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
   template void launch_extend_add<T>(const DevFronts&, const int32_t*, int, int, T*, T*, cudaStream_t);             \
   template void launch_potrf<T>(const DevFronts&, const int32_t*, int, int, T*, T*, int32_t*, cudaStream_t);       \
   template void launch_trsm<T>(const DevFronts&, const int32_t*, int, int, int, T*, const T*, int, cudaStream_t);  \
-  template void launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t); \
+  template void launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t,   \
+                                 int);                                                                             \
   template void launch_fwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, T*, int,     \
                                     cudaStream_t);                                                                 \
   template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, int,         \

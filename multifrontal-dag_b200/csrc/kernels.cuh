@@ -17,6 +17,29 @@ constexpr int kUpdTileSimt = 64;     // trailing-update output tile (FMA path)
 constexpr int kSolveB = kFactB;      // column step of the large-front solves (one inverted diagonal block)
 constexpr int kSolveRows = 256;      // rows per CTA of the backward large-front partial sums
 
+#ifdef __CUDACC__
+// Lower tile (ti, tj) of the trailing T x T tile grid (tile width tw) handled by
+// CTA x of an update launch.  mode 0: every lower tile (x enumerates the
+// triangle row by row); mode 1: only the tiles whose columns belong to the
+// next panel (the first kFactB columns: x = ti * (kFactB / tw) + tj); mode 2:
+// every other tile (x enumerates the triangle; next-panel tiles return).
+__device__ __forceinline__ bool select_tile(int mode, int T, int tw, int x, int& ti, int& tj) {
+  const int c1 = kFactB / tw;
+  if (mode == 1) {
+    ti = x / c1;
+    tj = x - ti * c1;
+    return ti < T && tj <= ti;
+  }
+  if (x >= T * (T + 1) / 2) return false;
+  int i = (int)((sqrtf(8.0f * (float)x + 1.0f) - 1.0f) * 0.5f);
+  while ((i + 1) * (i + 2) / 2 <= x) ++i;
+  while (i * (i + 1) / 2 > x) --i;
+  ti = i;
+  tj = x - i * (i + 1) / 2;
+  return mode == 0 || tj >= c1;
+}
+#endif
+
 // Opt every shared-memory-heavy kernel into the large dynamic shared memory
 // carve-out; called once per process before any launch or capture.
 cudaError_t prepare_kernels();
@@ -55,9 +78,17 @@ void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, 
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
                  const T* linv, int kind, cudaStream_t st);
+// Update tile subsets (select_tile): mode 0 all, 1 the next panel's columns, 2 the rest.
 template <typename T>
 void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, int tiles64, T* panel,
-                   T* upool, int kind, cudaStream_t st);
+                   T* upool, int kind, cudaStream_t st, int mode = 0);
+// FP32 trailing update on the tcgen05 tensor cores (update_tc.cu): split = 1 for 3xTF32, 0 for 1xTF32;
+// err[0] is raised if a bounded wait expires.
+cudaError_t prepare_update_tc();
+void launch_update_tc(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, float* panel,
+                      float* upool, int split, int32_t* err, cudaStream_t st, int mode = 0);
+// grid size of an update launch over `tiles` lower tiles of width tw in the given mode
+int update_grid(int tiles, int tw, int mode);
 
 // ---- solves --------------------------------------------------------------------
 template <typename T>

@@ -160,6 +160,20 @@ def test_update_kernel_variants_agree():
     del opts
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_lookahead_bitwise_equal(precision):
+    """The lookahead schedule (next panel's update tiles on the main stream,
+    the rest on a side stream) applies the same tile updates in the same order
+    per entry as the serial schedule: identical factors and solutions."""
+    p = P.laplace3d(16)
+    s0 = gpu_for(p, precision=precision, small_front_max=48)
+    s1 = gpu_for(p, precision=precision, small_front_max=48, reserved=(0, 1, 0, 0, 0, 0, 0))
+    x0, x1 = p.rhs.copy(), p.rhs.copy()
+    s0.solve(x0)
+    s1.solve(x1)
+    assert np.array_equal(x0, x1)
+
+
 def test_multiple_rhs():
     p = P.laplace2d(40)
     s = gpu_for(p)
@@ -220,6 +234,25 @@ def test_fp32_ir_reaches_1e12(mk):
     assert bwd <= 1e-12, bwd
     xo = oracle_for(p).solve(p.rhs)
     assert np.abs(x - xo).max() <= 1e-8 * np.abs(xo).max()
+
+
+@pytest.mark.parametrize("variant,tol", [(0, 3e-5), (2, 1e-2)], ids=["3xtf32", "1xtf32"])
+def test_fp32_tensor_update_against_ffma(variant, tol):
+    """The tcgen05 trailing update (0: 3xTF32, 2: 1xTF32) against the FFMA tiles
+    (1) on the same FP32 factorization: largest fronts' panels agree to the
+    TF32 rounding level, and refinement still reaches 1e-12."""
+    p = P.laplace3d(14)
+    ref = gpu_for(p, precision=H.MFD_PREC_FP32_IR, small_front_max=40, reserved=(1, 0, 0, 0, 0, 0, 0))
+    tc = gpu_for(p, precision=H.MFD_PREC_FP32_IR, small_front_max=40, reserved=(variant, 0, 0, 0, 0, 0, 0))
+    sym = oracle_for(p).symbolic()
+    nc = np.diff(sym["node_ptr"]); nr = np.diff(sym["lptr"])
+    for node in np.argsort(-(nc + nr))[:4] + 1:
+        f = int(nc[node - 1] + nr[node - 1]), int(nc[node - 1])
+        a, b = lower_panel(ref.front_panel(int(node)), *f), lower_panel(tc.front_panel(int(node)), *f)
+        assert np.abs(a - b).max() <= tol * np.abs(a).max(), node
+    x = p.rhs.copy()
+    rep, rc = tc.solve(x)
+    assert rc == 0 and rep.backward_error <= 1e-12
 
 
 # ---------------------------------------------------------------------------

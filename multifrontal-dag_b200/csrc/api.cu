@@ -167,7 +167,7 @@ struct mfd_handle {
 
   // device tables
   DBuf<int32_t> d_nc, d_nr, d_first, d_parent, d_child_ptr, d_child, d_lrow_off, d_lrow, d_local, d_a_beg, d_a_src,
-      d_a_pos, d_sidx, d_lists, d_perm, d_info;
+      d_a_pos, d_sidx, d_lists, d_perm, d_info, d_cnt;
   DBuf<int64_t> d_panel_off, d_u_off, d_v_off, d_s_off, d_d_off;
   DevFronts F{};
 
@@ -469,6 +469,8 @@ int upload_plan(mfd_handle* h) {
   CK(h->d_a_pos.alloc(h->nnz_total));
   CK(h->d_sidx.alloc(h->nnz_total));
   CK(h->d_info.alloc(2));   // [0] first bad pivot column, [1] bounded-wait expiry flag
+  CK(h->d_cnt.alloc(std::max(1, h->max_large_count)));   // backward-solve tickets, one per list slot
+  CK(cudaMemsetAsync(h->d_cnt.p, 0, sizeof(int32_t) * std::max(1, h->max_large_count), h->st));
   DevFronts& F = h->F;
   F.nc = h->d_nc.p; F.nr = h->d_nr.p; F.first = h->d_first.p; F.parent = h->d_parent.p;
   F.child_ptr = h->d_child_ptr.p; F.child = h->d_child.p; F.panel_off = h->d_panel_off.p; F.u_off = h->d_u_off.p;
@@ -867,7 +869,7 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       work(L.large, fl, by);
       record(h, st, MFD_K_SOLVE_LARGE, fl, by, [&] {
         launch_bwd_large<T>(F, lists + L.large.off, L.large.count, L.large.param2, L.large_max_nf, panel, dinv, X,
-                            ldx, V, S, nrhs, st, &n);
+                            ldx, V, S, h->d_cnt.p, nrhs, st, &n);
       });
     }
     for (const LaunchList& s : L.small) {

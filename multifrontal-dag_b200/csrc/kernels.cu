@@ -694,10 +694,24 @@ __device__ __forceinline__ T* trailing_addr(T* P, T* U, int nc, int nr, int nf, 
 
 // Trailing update on the FP64 tensor pipe: one 128x128 tile of the trailing
 // lower triangle per CTA, C -= P_i P_j^T over K = w <= 128 in chunks of 32,
-// double-buffered with cp.async; 8 warps as 2 (rows) x 4 (columns) of 64x32
-// (8x4 mma.m8n8k4.f64 each).  Shared-memory operands are k-major with a row
-// stride of 136 doubles, which makes the fragment loads conflict-free.
-constexpr int kUT = 128, kUK = 32, kULD = 136;
+// double-buffered with cp.async.  8 warps as 2 (rows) x 4 (columns) of 64x32,
+// each 4 x 4 mma.m16n8k16.f64 per K step of 16.  Shared-memory operands are
+// k-major with a row stride of 132 doubles (= 4 mod 16): every fragment load of
+// a half-warp hits 16 distinct 8-byte bank pairs.  The accumulators are loaded
+// with C itself (8 rows x 4 column pairs per warp access: full 32-byte
+// sectors) while the first operand chunk is in flight, the A fragments enter
+// negated, and the epilogue only stores.
+constexpr int kUT = 128, kUK = 32, kULD = 132;
+
+__device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32_t* list, int step, double* panel,
                                                         double* upool, int mode) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -715,14 +729,17 @@ __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32
   if (!select_tile(mode, T, kUT, blockIdx.x, ti, tj)) return;
   const int i0 = base + ti * kUT, j0 = base + tj * kUT;
   double* P = panel + F.panel_off[f];
+  double* U = upool + F.u_off[f];
   const int nchunks = (w + kUK - 1) / kUK;
+  const bool diag = ti == tj;
   auto load = [&](int stage, int kc) {
     double* dst = sm + stage * (2 * kUK * kULD);
-    for (int e = threadIdx.x; e < 2 * kUK * kUT; e += blockDim.x) {
-      int op = e / (kUK * kUT), rem = e - op * (kUK * kUT);
-      int k = rem / kUT, r = rem - k * kUT;
-      int row = (op == 0 ? i0 : j0) + r, col = kc * kUK + k;
-      bool valid = row < nf && col < w;
+    const int ops = diag ? 1 : 2;                       // a diagonal tile's B is its A
+    for (int e = threadIdx.x; e < ops * kUK * kUT; e += blockDim.x) {
+      const int op = e / (kUK * kUT), rem = e - op * (kUK * kUT);
+      const int k = rem / kUT, r = rem - k * kUT;
+      const int row = (op == 0 ? i0 : j0) + r, col = kc * kUK + k;
+      const bool valid = row < nf && col < w;
       const double* src = valid ? P + row + (size_t)(c0 + col) * nf : P;
       cp_async8(dst + op * (kUK * kULD) + k * kULD + r, src, valid);
     }
@@ -731,12 +748,20 @@ __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = warp >> 2, wn = warp & 3;
   const int g = lane >> 2, q = lane & 3;
-  double acc[8][4][2];
-#pragma unroll
-  for (int mi = 0; mi < 8; ++mi)
-#pragma unroll
-    for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+  // the accumulators start as C (loads in flight with the first operand chunk) and the
+  // A fragments enter negated, so the tile ends as C - P_i P_j^T and the epilogue only stores
+  const int rbase = i0 + wm * 64 + g, cbase = j0 + wn * 32 + 2 * q;
   load(0, 0);
+  double acc[4][4][4];
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int gi = rbase + mi * 16 + 8 * (e >> 1), gj = cbase + ni * 8 + (e & 1);
+        acc[mi][ni][e] = (gi < nf && gj < nf && gi >= gj) ? *trailing_addr(P, U, nc, nr, nf, gi, gj) : 0.0;
+      }
   for (int kc = 0; kc < nchunks; ++kc) {
     if (kc + 1 < nchunks) {
       load((kc + 1) & 1, kc + 1);
@@ -746,53 +771,34 @@ __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32
     }
     __syncthreads();
     const double* As = sm + (kc & 1) * (2 * kUK * kULD);
-    const double* Bs = As + kUK * kULD;
+    const double* Bs = diag ? As : As + kUK * kULD;
 #pragma unroll
-    for (int kk = 0; kk < kUK; kk += 4) {
-      double av[8], bv[4];
+    for (int kk = 0; kk < kUK; kk += 16) {
+      double bv[4][4];
 #pragma unroll
-      for (int mi = 0; mi < 8; ++mi) av[mi] = As[(kk + q) * kULD + wm * 64 + mi * 8 + g];
+      for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(kk + q) * kULD + wn * 32 + ni * 8 + g];
+        for (int i = 0; i < 4; ++i) bv[ni][i] = Bs[(kk + q + 4 * i) * kULD + wn * 32 + ni * 8 + g];
 #pragma unroll
-      for (int mi = 0; mi < 8; ++mi)
+      for (int mi = 0; mi < 4; ++mi) {
+        double av[8];
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], av[mi], bv[ni]);
+        for (int i = 0; i < 8; ++i) av[i] = -As[(kk + q + 4 * (i >> 1)) * kULD + wm * 64 + mi * 16 + g + 8 * (i & 1)];
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) dmma16(acc[mi][ni], av, bv[ni]);
+      }
     }
     __syncthreads();
   }
-  // Epilogue: stage P_i P_j^T in shared memory (the operand buffers are free
-  // now), then read-modify-write the tile column by column with coalesced,
-  // batched loads (all loads of a batch are issued before its stores).
-  constexpr int LDC = kUT + 1;
-  double* Cs = sm;
 #pragma unroll
-  for (int mi = 0; mi < 8; ++mi)
+  for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
-      for (int e = 0; e < 2; ++e)
-        Cs[(wm * 64 + mi * 8 + g) + (wn * 32 + ni * 8 + 2 * q + e) * LDC] = acc[mi][ni][e];
-  __syncthreads();
-  double* U = upool + F.u_off[f];
-  constexpr int kBatch = 8;
-  for (int e0 = threadIdx.x; e0 < kUT * kUT; e0 += kBatch * 256) {
-    double* addr[kBatch];
-    double val[kBatch];
-#pragma unroll
-    for (int b = 0; b < kBatch; ++b) {
-      const int e = e0 + b * 256;
-      const int r = e % kUT, c = e / kUT;
-      const int gi = i0 + r, gj = j0 + c;
-      addr[b] = (e < kUT * kUT && gi < nf && gj < nf && gi >= gj) ? trailing_addr(P, U, nc, nr, nf, gi, gj) : nullptr;
-      val[b] = addr[b] ? *addr[b] : 0.0;
-    }
-#pragma unroll
-    for (int b = 0; b < kBatch; ++b) {
-      const int e = e0 + b * 256;
-      if (addr[b]) *addr[b] = val[b] - Cs[(e % kUT) + (e / kUT) * LDC];
-    }
-  }
+      for (int e = 0; e < 4; ++e) {
+        const int gi = rbase + mi * 16 + 8 * (e >> 1), gj = cbase + ni * 8 + (e & 1);
+        if (gi < nf && gj < nf && gi >= gj) *trailing_addr(P, U, nc, nr, nf, gi, gj) = acc[mi][ni][e];
+      }
 }
 
 // Trailing update on the FMA pipes (any T): 64x64 tiles, K in chunks of 64,
@@ -940,6 +946,179 @@ __global__ void __launch_bounds__(256) k_bwd_small(DevFronts F, const int32_t* l
       __syncthreads();
     }
     for (int i = tid; i < nc; i += nt) X[first + i + r * ldx] = y[i];
+  }
+}
+
+// ---- fronts with nf <= 32: one warp per front ---------------------------------
+// Four fronts per 128-thread CTA.  The front is assembled in a per-warp
+// shared buffer (A entries, then the children's update matrices through
+// local_index), loaded one row per lane into registers and partially
+// factored there (nc pivots: shuffle for the pivot, rsqrt, rank-1 update with
+// the column broadcast through a double-buffered shared vector); the panel
+// columns and the update matrix are written back one column per step, lanes
+// over rows (coalesced).  No CTA-wide barrier: many more fronts in flight per
+// SM than the one-CTA-per-front kernel.
+constexpr int kWF = 32;          // front capacity of a warp
+constexpr int kWFLd = kWF + 1;
+constexpr int kWFWarps = 4;
+
+template <typename T>
+__device__ __forceinline__ T rsqrt_t(T x);
+template <>
+__device__ __forceinline__ double rsqrt_t<double>(double x) { return rsqrt(x); }
+template <>
+__device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
+
+template <typename T>
+__global__ void __launch_bounds__(kWFWarps * 32) k_small_warp(DevFronts F, const int32_t* list, int count,
+                                                              const double* __restrict__ a, T* __restrict__ panel,
+                                                              T* __restrict__ upool, int32_t* info) {
+  __shared__ T sbuf[kWFWarps][kWF * kWFLd];
+  __shared__ T cbuf[kWFWarps][2][kWF];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int slot = blockIdx.x * kWFWarps + warp;
+  if (slot >= count) return;
+  const int f = list[slot];
+  const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
+  T* S = sbuf[warp];
+  for (int e = lane; e < kWF * kWFLd; e += 32) S[e] = T(0);
+  __syncwarp();
+  const int a0 = F.a_beg[f], a1 = F.a_beg[f + 1];
+  for (int k = a0 + lane; k < a1; k += 32) {
+    const int pos = F.a_pos[k];
+    const int c = pos / nf, r = pos - c * nf;
+    S[r + c * kWFLd] = T(a[F.a_src[k]]);
+  }
+  __syncwarp();
+  for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
+    const int c = F.child[t];
+    const int nrc = F.nr[c];
+    const T* __restrict__ U = upool + F.u_off[c];
+    const int32_t* __restrict__ loc = F.local + F.lrow_off[c];
+    for (int e = lane; e < nrc * nrc; e += 32) {           // loc is injective: no two lanes hit one entry
+      const int j = e / nrc, i = e - j * nrc;
+      if (i >= j) S[(loc[i] - 1) + (loc[j] - 1) * kWFLd] += U[i + (size_t)j * nrc];
+    }
+    __syncwarp();
+  }
+  T row[kWF];
+#pragma unroll
+  for (int j = 0; j < kWF; ++j) row[j] = S[lane + j * kWFLd];
+  int bad = 0;
+#pragma unroll
+  for (int k = 0; k < kWF; ++k) {
+    if (k >= nc) break;
+    T d = __shfl_sync(0xffffffffu, row[k], k);
+    if (!(d > T(0))) {                    // uniform across the warp
+      if (!bad) bad = k + 1;
+      d = T(1);
+    }
+    const T y = rsqrt_t<T>(d);
+    const T l = row[k] * y;
+    T* cb = cbuf[warp][k & 1];
+    cb[lane] = l;
+    __syncwarp();
+    row[k] = lane == k ? d * y : l;
+#pragma unroll
+    for (int j = k + 1; j < kWF; ++j) row[j] -= l * cb[j];
+  }
+  if (bad && lane == 0) atomicMin(info, F.first[f] + bad);
+  T* P = panel + F.panel_off[f];
+  T* Uf = upool + F.u_off[f];
+#pragma unroll
+  for (int j = 0; j < kWF; ++j) {
+    if (j >= nf) break;
+    if (lane >= j && lane < nf) {
+      if (j < nc) P[lane + (size_t)j * nf] = row[j];
+      else Uf[(lane - nc) + (size_t)(j - nc) * nr] = row[j];
+    }
+  }
+}
+
+// forward solve of a warp front: v = own X + children's update vectors;
+// y = L11^{-1} v1 (lane i holds row i of the panel), v2 -= L21 y
+template <typename T>
+__global__ void __launch_bounds__(kWFWarps * 32) k_fwd_small_warp(DevFronts F, const int32_t* list, int count,
+                                                                  const T* __restrict__ panel, T* X, int64_t ldx,
+                                                                  T* V, int nrhs) {
+  __shared__ T vbuf[kWFWarps][kWF];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int slot = blockIdx.x * kWFWarps + warp;
+  if (slot >= count) return;
+  const int f = list[slot];
+  const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
+  const T* P = panel + F.panel_off[f];
+  T row[kWF];
+#pragma unroll
+  for (int j = 0; j < kWF; ++j) row[j] = (j < nc && lane < nf && lane >= j) ? P[lane + (size_t)j * nf] : T(0);
+  T dinv = T(1);
+#pragma unroll
+  for (int j = 0; j < kWF; ++j)
+    if (j == lane && j < nc) dinv = T(1) / row[j];
+  T* vs = vbuf[warp];
+  for (int r = 0; r < nrhs; ++r) {
+    vs[lane] = lane < nc ? X[first + lane + r * ldx] : T(0);
+    __syncwarp();
+    for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
+      const int c = F.child[t];
+      const int ncc = F.nc[c], nrc = F.nr[c];
+      const T* Vc = V + F.v_off[c] * nrhs + (int64_t)r * (ncc + nrc) + ncc;
+      const int32_t* loc = F.local + F.lrow_off[c];
+      if (lane < nrc) vs[loc[lane] - 1] += Vc[lane];
+      __syncwarp();
+    }
+    T v = vs[lane];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < kWF; ++k) {
+      if (k >= nc) break;
+      const T yk = __shfl_sync(0xffffffffu, v * dinv, k);
+      if (lane == k) v = yk;
+      else if (lane > k) v -= row[k] * yk;
+    }
+    if (lane < nc) X[first + lane + r * ldx] = v;
+    else if (lane < nf) V[F.v_off[f] * nrhs + (int64_t)r * nf + lane] = v;
+  }
+}
+
+// backward solve of a warp front: v2 = x(L rows); lane m < nc holds column m
+// of the panel: t_m = x_m - L21(:, m)^T v2, then L11^T x1 = t by shuffles
+template <typename T>
+__global__ void __launch_bounds__(kWFWarps * 32) k_bwd_small_warp(DevFronts F, const int32_t* list, int count,
+                                                                  const T* __restrict__ panel, T* X, int64_t ldx,
+                                                                  int nrhs) {
+  __shared__ T vbuf[kWFWarps][kWF];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int slot = blockIdx.x * kWFWarps + warp;
+  if (slot >= count) return;
+  const int f = list[slot];
+  const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
+  const int32_t* lr = F.lrow + F.lrow_off[f];
+  const T* P = panel + F.panel_off[f];
+  T col[kWF];                                // col[i] = L(i, lane) for i >= lane
+#pragma unroll
+  for (int i = 0; i < kWF; ++i) col[i] = (lane < nc && i >= lane && i < nf) ? P[i + (size_t)lane * nf] : T(0);
+  T dinv = T(1);
+#pragma unroll
+  for (int i = 0; i < kWF; ++i)
+    if (i == lane && i < nc) dinv = T(1) / col[i];
+  T* vs = vbuf[warp];
+  for (int r = 0; r < nrhs; ++r) {
+    vs[lane] = lane < nc ? X[first + lane + r * ldx] : (lane < nf ? X[lr[lane - nc] + r * ldx] : T(0));
+    __syncwarp();
+    T t = vs[lane];
+#pragma unroll
+    for (int i = 0; i < kWF; ++i)
+      if (i >= nc && i < nf) t -= col[i] * vs[i];
+    __syncwarp();
+#pragma unroll
+    for (int k = kWF - 1; k >= 0; --k) {
+      if (k >= nc) continue;
+      const T xk = __shfl_sync(0xffffffffu, t * dinv, k);
+      if (lane == k) t = xk;
+      else if (lane < k) t -= col[k] * xk;
+    }
+    if (lane < nc) X[first + lane + r * ldx] = t;
   }
 }
 
@@ -1212,6 +1391,123 @@ __global__ void __launch_bounds__(256) k_bwd_large_diag(DevFronts F, const int32
   }
 }
 
+// ---- fused backward step (one launch per panel step) -------------------------
+// Backward, any number of right-hand sides: every CTA writes its chunk's
+// partial sums; the last CTA of the front to finish (ticket on cnt[slot])
+// sums them in chunk order (deterministic), forms x_s = Li^T t_s, writes V_s
+// and X, and resets the ticket.  A front without rows below the block is
+// finished by CTA 0 alone.
+template <typename T>
+__global__ void __launch_bounds__(256) k_bwd_large_step(DevFronts F, const int32_t* list, int step,
+                                                        const T* __restrict__ panel, const T* __restrict__ dinv,
+                                                        T* X, int64_t ldx, T* V, T* scratch, int32_t* cnt,
+                                                        int nrhs) {
+  constexpr int CW = kSolveB / 8;
+  __shared__ T part[8][kBwdG][kSolveB];
+  __shared__ T ts[kSolveB];
+  __shared__ int last;
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kSolveB;
+  if (c0 >= nc) return;
+  const int w = min(kSolveB, nc - c0);
+  const int rs0 = c0 + w;
+  const int nchunks = nf > rs0 ? (nf - rs0 + kSolveRows - 1) / kSolveRows : 0;
+  const int rbase = rs0 + blockIdx.x * kSolveRows;
+  if ((int)blockIdx.x >= max(nchunks, 1)) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const T* P = panel + F.panel_off[f];
+  T* Vf = V + F.v_off[f] * nrhs;
+  if (nchunks > 0) {
+    const int i = rbase + warp * 32 + lane;
+    const bool valid = i < nf;
+    for (int r0 = 0; r0 < nrhs; r0 += kBwdG) {
+      const int g = min(kBwdG, nrhs - r0);
+      T xi[kBwdG];
+#pragma unroll
+      for (int u = 0; u < kBwdG; ++u) xi[u] = (valid && u < g) ? Vf[(int64_t)(r0 + u) * nf + i] : T(0);
+#pragma unroll 1
+      for (int kb = 0; kb < kSolveB; kb += 16) {
+        T pv[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) pv[j] = (valid && kb + j < w) ? P[i + (size_t)(c0 + kb + j) * nf] : T(0);
+#pragma unroll
+        for (int u = 0; u < kBwdG; ++u) {
+          if (u >= g) break;
+          T v[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] = pv[j] * xi[u];
+#pragma unroll
+          for (int s = 8; s >= 1; s >>= 1) {
+            const bool up = (lane & s) != 0;
+#pragma unroll
+            for (int j = 0; j < s; ++j) {
+              const T send = up ? v[j] : v[j + s];
+              const T keep = up ? v[j + s] : v[j];
+              v[j] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+            }
+          }
+          v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);
+          if (lane < 16) part[warp][u][kb + lane] = v[0];
+        }
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < g * kSolveB; e += blockDim.x) {
+        const int u = e / kSolveB, k = e % kSolveB;
+        T s = T(0);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) s += part[q][u][k];
+        scratch[F.s_off[f] * nrhs + ((int64_t)(r0 + u) * nchunks + blockIdx.x) * kSolveB + k] = s;
+      }
+      __syncthreads();
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&cnt[blockIdx.y], 1) == nchunks - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+  }
+  // finish: x_s = Li^T (v_s - sum of partials)
+  const T* Li = inv_block(F, dinv, f, step, blockIdx.y);
+  const int first = F.first[f];
+  T lc[CW][kSolveB / 32];
+#pragma unroll
+  for (int cc = 0; cc < CW; ++cc)
+#pragma unroll
+    for (int q = 0; q < kSolveB / 32; ++q) lc[cc][q] = Li[(lane + 32 * q) + (warp * CW + cc) * kSolveB];
+  for (int r = 0; r < nrhs; ++r) {
+    __syncthreads();
+    if (threadIdx.x < kSolveB) {
+      T s = T(0);
+      if (threadIdx.x < w) {
+        s = Vf[(int64_t)r * nf + c0 + threadIdx.x];
+        for (int q = 0; q < nchunks; ++q)      // other CTAs' partials: read past L1
+          s -= __ldcg(&scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + q) * kSolveB + threadIdx.x]);
+      }
+      ts[threadIdx.x] = s;
+    }
+    __syncthreads();
+    T tv[kSolveB / 32];
+#pragma unroll
+    for (int q = 0; q < kSolveB / 32; ++q) tv[q] = ts[lane + 32 * q];
+#pragma unroll
+    for (int cc = 0; cc < CW; ++cc) {
+      T s = T(0);
+#pragma unroll
+      for (int q = 0; q < kSolveB / 32; ++q) s += lc[cc][q] * tv[q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      const int i = warp * CW + cc;
+      if (lane == 0 && i < w) {
+        Vf[(int64_t)r * nf + c0 + i] = s;
+        X[first + c0 + i + r * ldx] = s;
+      }
+    }
+  }
+  if (nchunks > 0 && threadIdx.x == 0) cnt[blockIdx.y] = 0;
+}
+
 // ============================================================================
 // vectors
 // ============================================================================
@@ -1351,6 +1647,10 @@ template <typename T>
 void launch_small_fronts(const DevFronts& F, const int32_t* list, int count, int nf_max, const double* a, T* panel,
                          T* upool, int32_t* info, cudaStream_t st) {
   if (count <= 0) return;
+  if (nf_max <= kWF) {
+    k_small_warp<T><<<ceil_div(count, kWFWarps), kWFWarps * 32, 0, st>>>(F, list, count, a, panel, upool, info);
+    return;
+  }
   size_t sm = small_front_smem<T>(nf_max);
   set_smem(k_small_front<T>, sm);
   k_small_front<T><<<count, 256, sm, st>>>(F, list, a, panel, upool, info);
@@ -1429,6 +1729,10 @@ template <typename T>
 void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
                       int64_t ldx, T* V, int nrhs, cudaStream_t st) {
   if (count <= 0) return;
+  if (nf_max <= kWF) {
+    k_fwd_small_warp<T><<<ceil_div(count, kWFWarps), kWFWarps * 32, 0, st>>>(F, list, count, panel, X, ldx, V, nrhs);
+    return;
+  }
   size_t sm = fwd_small_smem<T>(nf_max);
   set_smem(k_fwd_small<T>, sm);
   k_fwd_small<T><<<count, 256, sm, st>>>(F, list, panel, X, ldx, V, nrhs);
@@ -1437,6 +1741,10 @@ template <typename T>
 void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
                       int64_t ldx, int nrhs, cudaStream_t st) {
   if (count <= 0) return;
+  if (nf_max <= kWF) {
+    k_bwd_small_warp<T><<<ceil_div(count, kWFWarps), kWFWarps * 32, 0, st>>>(F, list, count, panel, X, ldx, nrhs);
+    return;
+  }
   size_t sm = fwd_small_smem<T>(nf_max);
   set_smem(k_bwd_small<T>, sm);
   k_bwd_small<T><<<count, 256, sm, st>>>(F, list, panel, X, ldx, nrhs);
@@ -1456,17 +1764,15 @@ void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int ma
 }
 template <typename T>
 void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
-                      const T* dinv, T* X, int64_t ldx, T* V, T* scratch, int nrhs, cudaStream_t st,
+                      const T* dinv, T* X, int64_t ldx, T* V, T* scratch, int32_t* cnt, int nrhs, cudaStream_t st,
                       int64_t* launches) {
   if (count <= 0) return;
   k_bwd_large_gather<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
   const int steps = ceil_div(max_nc, kSolveB);
   const int chunks = std::max(1, ceil_div(max_nf, kSolveRows));
-  for (int s = steps - 1; s >= 0; --s) {
-    k_bwd_large_rest<T><<<dim3(chunks, count), 256, 0, st>>>(F, list, s, panel, V, scratch, nrhs);
-    k_bwd_large_diag<T><<<count, 256, 0, st>>>(F, list, s, dinv, X, ldx, V, scratch, nrhs);
-  }
-  if (launches) *launches += 1 + 2 * steps;
+  for (int s = steps - 1; s >= 0; --s)
+    k_bwd_large_step<T><<<dim3(chunks, count), 256, 0, st>>>(F, list, s, panel, dinv, X, ldx, V, scratch, cnt, nrhs);
+  if (launches) *launches += 1 + steps;
 }
 
 template <typename T>
@@ -1524,7 +1830,7 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
   template void launch_fwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
                                     int64_t, T*, int, cudaStream_t, int64_t*);                                     \
   template void launch_bwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
-                                    int64_t, T*, T*, int, cudaStream_t, int64_t*);                                 \
+                                    int64_t, T*, T*, int32_t*, int, cudaStream_t, int64_t*);                       \
   template void launch_permute_in<T>(const double*, int64_t, const int32_t*, T*, int64_t, int64_t, int,            \
                                      cudaStream_t);                                                                \
   template void launch_permute_out<T>(const T*, int64_t, const int32_t*, double*, int64_t, int64_t, int,           \

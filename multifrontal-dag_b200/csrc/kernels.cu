@@ -39,6 +39,16 @@ __device__ __forceinline__ float dev_sqrt<float>(float x) { return sqrtf(x); }
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc, bool valid) {
+
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+  int sz = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
 // Strided element loop (e = threadIdx.x, += blockDim.x, e < total) whose
 // global loads are issued kBatch at a time before the matching stores, so a
 // thread keeps kBatch independent loads in flight instead of one.
@@ -460,7 +470,22 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   T* P = panel + F.panel_off[f];
   // ---- load the lower w x w block, identity on the padding ----
-  batched_loop(
+  if constexpr (sizeof(T) == 8) {
+    // asynchronous 8-byte copies, all in flight at once; out-of-block entries zero-filled
+    for (int e = tid; e < B * B; e += kPotrfThreads) {
+      const int i = e % B, j = e / B;
+      if (i < wp && j < wp) {
+        if (i == j && i >= w) {
+          S[i + j * kPLd] = 1.0;              // identity on the padded diagonal
+        } else {
+          const bool v = i < w && j < w && i >= j;
+          cp_async8(&S[i + j * kPLd], v ? (const void*)&P[(c0 + i) + (size_t)(c0 + j) * nf] : (const void*)P, v);
+        }
+      }
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+  } else batched_loop(
       B * B,
       [&](int e) {
         const int i = e % B, j = e / B;
@@ -561,130 +586,6 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
   }
 }
 
-__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc, bool valid) {
-
-  unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
-  int sz = valid ? 8 : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(sz));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
-
-
-// TRSM on the FP64 tensor pipe: 64 rows x w columns of the panel per CTA,
-// X = A Li^T with Li = L11^{-1}; 8 warps as 2 (rows) x 4 (columns) of 32x32.
-constexpr int kTrRows = 64, kTrLdA = 72, kTrLdB = 136;
-__global__ void __launch_bounds__(256, 1) k_trsm_dmma(DevFronts F, const int32_t* list, int step, double* panel,
-                                                      const double* linv) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* As = reinterpret_cast<double*>(smem_raw);      // [k][row], k < 128
-  double* Bs = As + kFactB * kTrLdA;                      // [k][n]
-  const int f = list[blockIdx.y];
-  const int nc = F.nc[f], nf = nc + F.nr[f];
-  const int c0 = step * kFactB;
-  if (c0 >= nc) return;
-  const int w = min(kFactB, nc - c0);
-  const int r0 = c0 + w + blockIdx.x * kTrRows;
-  if (r0 >= nf) return;
-  double* P = panel + F.panel_off[f];
-  const double* Li = inv_block(F, linv, f, step, blockIdx.y);
-  const int wp = (w + 3) & ~3;
-  batched_loop(
-      kTrRows * wp,
-      [&](int e) {
-        const int k = e / kTrRows, r = e - k * kTrRows;
-        return (k < w && r0 + r < nf) ? P[(r0 + r) + (size_t)(c0 + k) * nf] : 0.0;
-      },
-      [&](int e, double v) { As[(e / kTrRows) * kTrLdA + (e % kTrRows)] = v; });
-  batched_loop(
-      kFactB * wp, [&](int e) { return Li[(e % kFactB) + (e / kFactB) * kFactB]; },
-      [&](int e, double v) { Bs[(e / kFactB) * kTrLdB + (e % kFactB)] = v; });
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wm = warp >> 2, wn = warp & 3;
-  const int g = lane >> 2, q = lane & 3;
-  double acc[4][4][2];
-#pragma unroll
-  for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-    for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
-  for (int kk = 0; kk < wp; kk += 4) {
-    double av[4], bv[4];
-#pragma unroll
-    for (int mi = 0; mi < 4; ++mi) av[mi] = As[(kk + q) * kTrLdA + wm * 32 + mi * 8 + g];
-#pragma unroll
-    for (int ni = 0; ni < 4; ++ni) bv[ni] = Bs[(kk + q) * kTrLdB + wn * 32 + ni * 8 + g];
-#pragma unroll
-    for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], av[mi], bv[ni]);
-  }
-#pragma unroll
-  for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-    for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        int gi = r0 + wm * 32 + mi * 8 + g;
-        int n = wn * 32 + ni * 8 + 2 * q + e;
-        if (gi < nf && n < w) P[gi + (size_t)(c0 + n) * nf] = acc[mi][ni][e];
-      }
-}
-
-// TRSM on the FMA pipes (any T): 64 rows x w columns, thread = 4 rows x 8 columns.
-template <typename T>
-__global__ void __launch_bounds__(256) k_trsm_simt(DevFronts F, const int32_t* list, int step, T* panel,
-                                                   const T* linv) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int LDA = kTrRows + 4, LDB = kFactB + 4;
-  T* As = reinterpret_cast<T*>(smem_raw);
-  T* Bs = As + kFactB * LDA;
-  const int f = list[blockIdx.y];
-  const int nc = F.nc[f], nf = nc + F.nr[f];
-  const int c0 = step * kFactB;
-  if (c0 >= nc) return;
-  const int w = min(kFactB, nc - c0);
-  const int r0 = c0 + w + blockIdx.x * kTrRows;
-  if (r0 >= nf) return;
-  T* P = panel + F.panel_off[f];
-  const T* Li = inv_block(F, linv, f, step, blockIdx.y);
-  batched_loop(
-      kTrRows * w,
-      [&](int e) {
-        const int k = e / kTrRows, r = e - k * kTrRows;
-        return (r0 + r < nf) ? P[(r0 + r) + (size_t)(c0 + k) * nf] : T(0);
-      },
-      [&](int e, T v) { As[(e / kTrRows) * LDA + (e % kTrRows)] = v; });
-  batched_loop(
-      kFactB * w, [&](int e) { return Li[(e % kFactB) + (e / kFactB) * kFactB]; },
-      [&](int e, T v) { Bs[(e / kFactB) * LDB + (e % kFactB)] = v; });
-  __syncthreads();
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  T acc[4][8];
-#pragma unroll
-  for (int m = 0; m < 4; ++m)
-#pragma unroll
-    for (int n = 0; n < 8; ++n) acc[m][n] = T(0);
-  for (int k = 0; k < w; ++k) {
-    T av[4], bv[8];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) av[m] = As[k * LDA + ty + 16 * m];
-#pragma unroll
-    for (int n = 0; n < 8; ++n) bv[n] = Bs[k * LDB + tx + 16 * n];
-#pragma unroll
-    for (int m = 0; m < 4; ++m)
-#pragma unroll
-      for (int n = 0; n < 8; ++n) acc[m][n] += av[m] * bv[n];
-  }
-#pragma unroll
-  for (int m = 0; m < 4; ++m)
-#pragma unroll
-    for (int n = 0; n < 8; ++n) {
-      int gi = r0 + ty + 16 * m, c = tx + 16 * n;
-      if (gi < nf && c < w) P[gi + (size_t)(c0 + c) * nf] = acc[m][n];
-    }
-}
 
 
 template <typename T>
@@ -710,6 +611,106 @@ __device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[8], con
       : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
         "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
+// Panel TRSM X = A Li^T (Li = L11^{-1}, lower): one CTA per 32 rows of X and
+// all its w <= 128 columns (the TRSM is in place, so a CTA must read its rows
+// of A before any CTA writes them: rows are never split across CTAs), so a
+// panel step of nrem rows runs on nrem / 32 CTAs.  Operands arrive by
+// cp.async (all in flight at once).  FP64: 8 warps as 2 x 4 of 16 x 32
+// (m16n8k16 DMMA); FP32: 256 threads of 2 rows x 8 columns (FFMA).
+constexpr int kTr2Rows = 32;
+constexpr int kTr2LdA = kTr2Rows + 4, kTr2LdB = kFactB + 4;   // = 4 mod 16 doubles
+template <typename T>
+constexpr size_t trsm2_smem() {
+  return ((size_t)kFactB * kTr2LdA + (size_t)kFactB * kTr2LdB) * sizeof(T);
+}
+
+template <typename T>
+__device__ __forceinline__ void cp_async_t(T* dst, const T* src, bool valid) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+  const int sz = valid ? (int)sizeof(T) : 0;
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src), "r"(sz));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(src), "r"(sz));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_trsm2(DevFronts F, const int32_t* list, int step, T* panel, const T* linv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);            // [k][row]
+  T* Bs = As + kFactB * kTr2LdA;                      // [k][n]: Li(n, k)
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kFactB;
+  if (c0 >= nc) return;
+  const int w = min(kFactB, nc - c0);
+  const int r0 = c0 + w + blockIdx.x * kTr2Rows;
+  if (r0 >= nf) return;
+  T* P = panel + F.panel_off[f];
+  const T* Li = inv_block(F, linv, f, step, blockIdx.y);
+  const int kp = (w + 15) & ~15;
+  for (int e = threadIdx.x; e < kTr2Rows * kp; e += blockDim.x) {
+    const int k = e / kTr2Rows, r = e - k * kTr2Rows;
+    const bool v = k < w && r0 + r < nf;
+    cp_async_t(&As[k * kTr2LdA + r], v ? P + (r0 + r) + (size_t)(c0 + k) * nf : P, v);
+  }
+  for (int e = threadIdx.x; e < kFactB * kp; e += blockDim.x) {
+    const int k = e / kFactB, n = e - k * kFactB;
+    const bool v = k < w && n < w;
+    cp_async_t(&Bs[k * kTr2LdB + n], v ? Li + n + (size_t)k * kFactB : Li, v);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  if constexpr (sizeof(T) == 8) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = warp >> 2, wn = warp & 3;            // 16-row band, 32-column band
+    const int g = lane >> 2, q = lane & 3;
+    double acc[4][4] = {};
+    for (int kk = 0; kk < kp; kk += 16) {
+      double av[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) av[i] = As[(kk + q + 4 * (i >> 1)) * kTr2LdA + wm * 16 + g + 8 * (i & 1)];
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        double bv[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) bv[i] = Bs[(kk + q + 4 * i) * kTr2LdB + wn * 32 + ni * 8 + g];
+        dmma16(acc[ni], av, bv);
+      }
+    }
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int gi = r0 + wm * 16 + g + 8 * (e >> 1);
+        const int n = wn * 32 + ni * 8 + 2 * q + (e & 1);
+        if (gi < nf && n < w) P[gi + (size_t)(c0 + n) * nf] = acc[ni][e];
+      }
+  } else {
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // columns tx + 16 m, rows ty + 16 l
+    T acc[2][8] = {};
+    for (int k = 0; k < w; ++k) {
+      T av[2], bv[8];
+#pragma unroll
+      for (int l = 0; l < 2; ++l) av[l] = As[k * kTr2LdA + ty + 16 * l];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) bv[m] = Bs[k * kTr2LdB + tx + 16 * m];
+#pragma unroll
+      for (int l = 0; l < 2; ++l)
+#pragma unroll
+        for (int m = 0; m < 8; ++m) acc[l][m] = fmaf(av[l], bv[m], acc[l][m]);
+    }
+#pragma unroll
+    for (int l = 0; l < 2; ++l)
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const int gi = r0 + ty + 16 * l, n = tx + 16 * m;
+        if (gi < nf && n < w) P[gi + (size_t)(c0 + n) * nf] = acc[l][m];
+      }
+  }
 }
 
 __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32_t* list, int step, double* panel,
@@ -1612,7 +1613,7 @@ cudaError_t prepare_kernels() {
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t r) { if (r != cudaSuccess && e == cudaSuccess) e = r; };
   chk(opt_in(k_small_front<double>)); chk(opt_in(k_small_front<float>));
-  chk(opt_in(k_trsm_dmma)); chk(opt_in(k_trsm_simt<double>)); chk(opt_in(k_trsm_simt<float>));
+  chk(opt_in(k_trsm2<double>)); chk(opt_in(k_trsm2<float>));
   chk(opt_in(k_update_dmma));
   chk(opt_in(k_potrf<double>)); chk(opt_in(k_potrf<float>));
   chk(prepare_update_tc());
@@ -1686,17 +1687,10 @@ template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
                  const T* linv, int kind, cudaStream_t st) {
   if (count <= 0 || row_blocks <= 0) return;
-  dim3 grid(row_blocks, count);
-  if constexpr (sizeof(T) == 8) {
-    if (kind == 0) {
-      size_t sm = ((size_t)kFactB * kTrLdA + (size_t)kFactB * kTrLdB) * sizeof(double);
-      k_trsm_dmma<<<grid, 256, sm, st>>>(F, list, step, reinterpret_cast<double*>(panel),
-                                         reinterpret_cast<const double*>(linv));
-      return;
-    }
-  }
-  size_t sm = ((size_t)kFactB * (kTrRows + 4) + (size_t)kFactB * (kFactB + 4)) * sizeof(T);
-  k_trsm_simt<T><<<grid, 256, sm, st>>>(F, list, step, panel, linv);
+  (void)kind;
+  // row_blocks counts 64-row blocks
+  dim3 grid(row_blocks * 2, count);
+  k_trsm2<T><<<grid, 256, trsm2_smem<T>(), st>>>(F, list, step, panel, linv);
 }
 int update_grid(int tiles, int tw, int mode) {
   if (mode != 1) return tiles;

@@ -145,6 +145,26 @@ def test_laplace3d_fp64_large_path(small_max):
         assert np.abs(got - ref).max() <= FACTOR_TOL * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_wide_panels_many_rows(precision):
+    """22^3 Laplacian with large relaxed supernodes (max_zero 1000): fronts with
+    several full 128-column panel steps and hundreds of rows below them, the
+    shape where a panel step's POTRF, TRSM and trailing-update CTAs work on
+    the same columns."""
+    p = P.laplace3d(22)
+    s = gpu_for(p, max_zero=1000, precision=precision)
+    assert s.stats().max_front > 3 * 128
+    x = p.rhs.copy()
+    rep, rc = s.solve(x)
+    assert rc == 0
+    bwd = P.backward_error(p.n, p.col, p.row, p.val, x, p.rhs)
+    assert bwd <= FP64_BWD_TOL, bwd
+    if precision == 1:
+        assert rep.iterations <= 3, rep.iterations
+    xo = oracle_for(p, max_zero=1000).solve(p.rhs)
+    assert np.abs(x - xo).max() <= 1e-9 * np.abs(xo).max()
+
+
 def test_update_kernel_variants_agree():
     """DMMA and FFMA trailing updates give the same factor to rounding."""
     p = P.laplace3d(14)

@@ -760,6 +760,10 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
     // rest of the trailing update on the side stream, so POTRF/TRSM of step
     // s+1 overlap it; the next step's update waits for it (shared columns).
     const bool lookahead = h->opt.reserved[1] != 1 && !h->profiling;
+    // programmatic dependent launch along the panel chain: opt-in (reserved[2] = 1).
+    // Measured on the 64^3 Laplacian it costs 1-2 ms (early-launched CTAs wait on
+    // SMs the side-stream update could use), so the default leaves it off.
+    const bool pdl = h->opt.reserved[2] == 1 && !h->profiling;
     bool pending = false;
     for (size_t s = 0; s < L.steps.size(); ++s) {
       const LaunchList& p = L.steps[s];
@@ -780,20 +784,22 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
           ub1 += w * (2.0 * (n1 * (n1 + 1) / 2 + (nrem - n1) * n1) + 2.0 * nrem * wd);
         }
       record(h, st, MFD_K_PANEL, pf, pb,
-             [&] { launch_potrf<T>(F, lists + p.off, p.count, (int)s, panel, diag, h->d_info.p, st); });
-      record(h, st, MFD_K_TRSM, tf, tb,
-             [&] { launch_trsm<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, kind == 1 ? 1 : 0, st); });
+             [&] { launch_potrf<T>(F, lists + p.off, p.count, (int)s, panel, diag, h->d_info.p, st, pdl); });
+      record(h, st, MFD_K_TRSM, tf, tb, [&] {
+        launch_trsm<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, kind == 1 ? 1 : 0, st, pdl);
+      });
       n += 2;
       auto update = [&](cudaStream_t us, int mode) {
+        const bool upd_pdl = pdl && us == st;        // right behind the TRSM on the main stream
         if constexpr (sizeof(T) == 4) {
           if (kind == 0 || kind == 2) {
             launch_update_tc(F, lists + p.off, p.count, (int)s, p.param2, reinterpret_cast<float*>(panel),
-                             reinterpret_cast<float*>(upool), kind == 0 ? 1 : 0, h->d_info.p + 1, us, mode);
+                             reinterpret_cast<float*>(upool), kind == 0 ? 1 : 0, h->d_info.p + 1, us, mode, upd_pdl);
             return;
           }
         }
         launch_update<T>(F, lists + p.off, p.count, (int)s, p.param2, p.param3, panel, upool, kind == 1 ? 1 : 0, us,
-                         mode);
+                         mode, upd_pdl && kind != 1);
       };
       if (pending) cudaStreamWaitEvent(st, h->ev_join, 0);
       pending = false;

@@ -469,6 +469,8 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
   const int nsb = (w + kPSub - 1) / kPSub, wp = nsb * kPSub;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   T* P = panel + F.panel_off[f];
+  pdl_wait();
+  pdl_trigger();          // after the wait: every kernel before this one has completed
   // ---- load the lower w x w block, identity on the padding ----
   if constexpr (sizeof(T) == 8) {
     // asynchronous 8-byte copies, all in flight at once; out-of-block entries zero-filled
@@ -651,11 +653,15 @@ __global__ void __launch_bounds__(256) k_trsm2(DevFronts F, const int32_t* list,
   T* P = panel + F.panel_off[f];
   const T* Li = inv_block(F, linv, f, step, blockIdx.y);
   const int kp = (w + 15) & ~15;
+  // the rows below the diagonal block do not depend on the POTRF that precedes this kernel
+  // (no event wait sits between the two launches)
   for (int e = threadIdx.x; e < kTr2Rows * kp; e += blockDim.x) {
     const int k = e / kTr2Rows, r = e - k * kTr2Rows;
     const bool v = k < w && r0 + r < nf;
     cp_async_t(&As[k * kTr2LdA + r], v ? P + (r0 + r) + (size_t)(c0 + k) * nf : P, v);
   }
+  pdl_wait();
+  pdl_trigger();
   for (int e = threadIdx.x; e < kFactB * kp; e += blockDim.x) {
     const int k = e / kFactB, n = e - k * kFactB;
     const bool v = k < w && n < w;
@@ -752,7 +758,10 @@ __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32
   // the accumulators start as C (loads in flight with the first operand chunk) and the
   // A fragments enter negated, so the tile ends as C - P_i P_j^T and the epilogue only stores
   const int rbase = i0 + wm * 64 + g, cbase = j0 + wn * 32 + 2 * q;
-  load(0, 0);
+  // C may be written by a kernel this one waits on through an event (the
+  // lookahead's side stream): everything is read after the wait
+  pdl_wait();
+  pdl_trigger();
   double acc[4][4][4];
 #pragma unroll
   for (int mi = 0; mi < 4; ++mi)
@@ -763,6 +772,7 @@ __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32
         const int gi = rbase + mi * 16 + 8 * (e >> 1), gj = cbase + ni * 8 + (e & 1);
         acc[mi][ni][e] = (gi < nf && gj < nf && gi >= gj) ? *trailing_addr(P, U, nc, nr, nf, gi, gj) : 0.0;
       }
+  load(0, 0);
   for (int kc = 0; kc < nchunks; ++kc) {
     if (kc + 1 < nchunks) {
       load((kc + 1) & 1, kc + 1);
@@ -1679,18 +1689,18 @@ void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int m
 }
 template <typename T>
 void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
-                  cudaStream_t st) {
+                  cudaStream_t st, bool pdl) {
   if (count <= 0) return;
-  k_potrf<T><<<count, kPotrfThreads, kPotrfSmem, st>>>(F, list, step, panel, linv, info);
+  launch_k(k_potrf<T>, dim3(count), dim3(kPotrfThreads), kPotrfSmem, st, pdl, F, list, step, panel, linv, info);
 }
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
-                 const T* linv, int kind, cudaStream_t st) {
+                 const T* linv, int kind, cudaStream_t st, bool pdl) {
   if (count <= 0 || row_blocks <= 0) return;
   (void)kind;
   // row_blocks counts 64-row blocks
   dim3 grid(row_blocks * 2, count);
-  k_trsm2<T><<<grid, 256, trsm2_smem<T>(), st>>>(F, list, step, panel, linv);
+  launch_k(k_trsm2<T>, grid, dim3(256), trsm2_smem<T>(), st, pdl, F, list, step, panel, linv);
 }
 int update_grid(int tiles, int tw, int mode) {
   if (mode != 1) return tiles;
@@ -1701,15 +1711,15 @@ int update_grid(int tiles, int tw, int mode) {
 
 template <typename T>
 void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, int tiles64, T* panel,
-                   T* upool, int kind, cudaStream_t st, int mode) {
+                   T* upool, int kind, cudaStream_t st, int mode, bool pdl) {
   if (count <= 0) return;
   if constexpr (sizeof(T) == 8) {
     if (kind == 0) {
       const int g = update_grid(tiles128, kUT, mode);
       if (g <= 0) return;
       size_t sm = 2 * 2 * (size_t)kUK * kULD * sizeof(double);
-      k_update_dmma<<<dim3(g, count), 256, sm, st>>>(F, list, step, reinterpret_cast<double*>(panel),
-                                                      reinterpret_cast<double*>(upool), mode);
+      launch_k(k_update_dmma, dim3(g, count), dim3(256), sm, st, pdl, F, list, step, reinterpret_cast<double*>(panel),
+               reinterpret_cast<double*>(upool), mode);
       return;
     }
   }
@@ -1813,10 +1823,11 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
   template void launch_assemble_large<T>(const DevFronts&, const int32_t*, int, int, const double*, T*,             \
                                          cudaStream_t);                                                            \
   template void launch_extend_add<T>(const DevFronts&, const int32_t*, int, int, T*, T*, cudaStream_t);             \
-  template void launch_potrf<T>(const DevFronts&, const int32_t*, int, int, T*, T*, int32_t*, cudaStream_t);       \
-  template void launch_trsm<T>(const DevFronts&, const int32_t*, int, int, int, T*, const T*, int, cudaStream_t);  \
+  template void launch_potrf<T>(const DevFronts&, const int32_t*, int, int, T*, T*, int32_t*, cudaStream_t, bool); \
+  template void launch_trsm<T>(const DevFronts&, const int32_t*, int, int, int, T*, const T*, int, cudaStream_t,   \
+                               bool);                                                                              \
   template void launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t,   \
-                                 int);                                                                             \
+                                 int, bool);                                                                       \
   template void launch_fwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, T*, int,     \
                                     cudaStream_t);                                                                 \
   template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, int,         \

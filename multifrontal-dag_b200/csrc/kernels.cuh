@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <utility>
 
 #include "plan.hpp"
 
@@ -40,6 +41,32 @@ __device__ __forceinline__ bool select_tile(int mode, int T, int tw, int x, int&
 }
 #endif
 
+// Programmatic dependent launch: a kernel launched with `pdl` may start while
+// the previous kernel of its stream is still running; it calls pdl_wait()
+// before touching anything that kernel writes (work that does not depend on
+// it goes first), and pdl_trigger(), always issued after pdl_wait() so that
+// every older kernel has completed, lets the next kernel start early.  Both
+// are no-ops for a kernel launched without the attribute.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+#endif
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, bool pdl,
+                     Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // Opt every shared-memory-heavy kernel into the large dynamic shared memory
 // carve-out; called once per process before any launch or capture.
 cudaError_t prepare_kernels();
@@ -74,19 +101,19 @@ void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int m
 //   update : trailing lower triangle -= P P^T                  (kind 0: DMMA 128-tiles, 1: FMA 64-tiles)
 template <typename T>
 void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
-                  cudaStream_t st);
+                  cudaStream_t st, bool pdl = false);
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
-                 const T* linv, int kind, cudaStream_t st);
+                 const T* linv, int kind, cudaStream_t st, bool pdl = false);
 // Update tile subsets (select_tile): mode 0 all, 1 the next panel's columns, 2 the rest.
 template <typename T>
 void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, int tiles64, T* panel,
-                   T* upool, int kind, cudaStream_t st, int mode = 0);
+                   T* upool, int kind, cudaStream_t st, int mode = 0, bool pdl = false);
 // FP32 trailing update on the tcgen05 tensor cores (update_tc.cu): split = 1 for 3xTF32, 0 for 1xTF32;
 // err[0] is raised if a bounded wait expires.
 cudaError_t prepare_update_tc();
 void launch_update_tc(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, float* panel,
-                      float* upool, int split, int32_t* err, cudaStream_t st, int mode = 0);
+                      float* upool, int split, int32_t* err, cudaStream_t st, int mode = 0, bool pdl = false);
 // grid size of an update launch over `tiles` lower tiles of width tw in the given mode
 int update_grid(int tiles, int tw, int mode);
 

@@ -156,6 +156,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_update_tc(DevFronts F, const 
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = *tslot;
+  pdl_wait();                       // the panel rows are the preceding TRSM's output
+  pdl_trigger();
 
   const int nch = (w + kTcK - 1) / kTcK;
   bool ok = true;
@@ -267,10 +269,11 @@ cudaError_t prepare_update_tc() {
 }
 
 void launch_update_tc(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, float* panel,
-                      float* upool, int split, int32_t* err, cudaStream_t st, int mode) {
+                      float* upool, int split, int32_t* err, cudaStream_t st, int mode, bool pdl) {
   const int g = update_grid(tiles128, kTcTile, mode);
   if (count <= 0 || g <= 0) return;
-  k_update_tc<<<dim3(g, count), kTcThreads, kTcSmem, st>>>(F, list, step, panel, upool, split, err, mode);
+  launch_k(k_update_tc, dim3(g, count), dim3(kTcThreads), kTcSmem, st, pdl, F, list, step, panel, upool, split, err,
+           mode);
 }
 
 }  // namespace mfd

@@ -194,6 +194,18 @@ def test_lookahead_bitwise_equal(precision):
     assert np.array_equal(x0, x1)
 
 
+def test_programmatic_launch_matches():
+    """Programmatic dependent launch along the panel chain (opt-in) gives the
+    same factor as the default schedule."""
+    p = P.laplace3d(22)
+    s0 = gpu_for(p, max_zero=1000)
+    s1 = gpu_for(p, max_zero=1000, reserved=(0, 0, 1, 0, 0, 0, 0))
+    x0, x1 = p.rhs.copy(), p.rhs.copy()
+    s0.solve(x0)
+    s1.solve(x1)
+    assert np.array_equal(x0, x1)
+
+
 def test_multiple_rhs():
     p = P.laplace2d(40)
     s = gpu_for(p)

@@ -49,6 +49,16 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+template <typename T>
+__device__ __forceinline__ void cp_async_t(T* dst, const T* src, bool valid) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+  const int sz = valid ? (int)sizeof(T) : 0;
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src), "r"(sz));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(src), "r"(sz));
+}
+
 // Strided element loop (e = threadIdx.x, += blockDim.x, e < total) whose
 // global loads are issued kBatch at a time before the matching stores, so a
 // thread keeps kBatch independent loads in flight instead of one.
@@ -487,22 +497,22 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
     }
     cp_async_commit();
     cp_async_wait<0>();
-  } else batched_loop(
-      B * B,
-      [&](int e) {
-        const int i = e % B, j = e / B;
-        double v = 0.0;
-        if (i < w && j < w) {
-          if (i >= j) v = (double)P[(c0 + i) + (size_t)(c0 + j) * nf];
-        } else if (i == j) {
-          v = 1.0;
-        }
-        return v;
-      },
-      [&](int e, double v) {
-        const int i = e % B, j = e / B;
-        if (i < wp && j < wp) S[i + j * kPLd] = v;
-      });
+  } else {
+    // FP32 storage: 4-byte copies into a float staging block (the D / Y / rq /
+    // cbuf area, 66 KB, is free until the first sub-block), then widened into S
+    float* Fs = reinterpret_cast<float*>(Dv);
+    for (int e = tid; e < B * B; e += kPotrfThreads) {
+      const int i = e % B, j = e / B;
+      if (i < w && j < w && i >= j) cp_async_t(&Fs[e], (const float*)&P[(c0 + i) + (size_t)(c0 + j) * nf], true);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    for (int e = tid; e < B * B; e += kPotrfThreads) {
+      const int i = e % B, j = e / B;
+      if (i < wp && j < wp) S[i + j * kPLd] = (i < w && j < w) ? (i >= j ? (double)Fs[e] : 0.0) : (i == j ? 1.0 : 0.0);
+    }
+  }
   __syncthreads();
   // ---- right-looking over 32-wide sub-blocks ----
   for (int b = 0; b < nsb; ++b) {
@@ -628,15 +638,6 @@ constexpr size_t trsm2_smem() {
   return ((size_t)kFactB * kTr2LdA + (size_t)kFactB * kTr2LdB) * sizeof(T);
 }
 
-template <typename T>
-__device__ __forceinline__ void cp_async_t(T* dst, const T* src, bool valid) {
-  unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
-  const int sz = valid ? (int)sizeof(T) : 0;
-  if constexpr (sizeof(T) == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src), "r"(sz));
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(src), "r"(sz));
-}
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_trsm2(DevFronts F, const int32_t* list, int step, T* panel, const T* linv) {

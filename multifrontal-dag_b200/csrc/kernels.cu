@@ -1136,51 +1136,29 @@ __global__ void __launch_bounds__(kWFWarps * 32) k_bwd_small_warp(DevFronts F, c
 
 // ---- large fronts: the solve vector of front f lives in V (nf per RHS) --------
 // Panel steps of kSolveB = 128 columns use the inverted diagonal blocks kept
-// from the factorization (Li = L_ss^{-1}), so a step is two GEMV/GEMM-shaped
-// launches and no sequential column loop:
-//   forward : y_s = Li v_s (k_fwd_large_diag), v_rest -= L_rest,s y_s (k_fwd_large_rest)
-//   backward: t_s = v_s - L_rest,s^T x_rest (k_bwd_large_rest partial sums per
-//             256-row chunk, summed in chunk order: deterministic), x_s = Li^T t_s
-//             (k_bwd_large_diag)
-// The diag kernels write the front's own entries of X directly.
+// from the factorization (Li = L_ss^{-1}), one launch per step:
+//   forward : v_rest -= L_rest,s y_s over 32-row chunks (k_fwd_large_rest);
+//             the last CTA of the front to finish (ticket) then forms the next
+//             step's y_{s+1} = Li v_{s+1}; y_0 is formed by the gather kernel
+//   backward: t_s = v_s - L_rest,s^T x_rest, partial sums per 256-row chunk;
+//             the last CTA sums them in chunk order (deterministic) and forms
+//             x_s = Li^T t_s (k_bwd_large_step)
+// The diagonal solves write the front's own entries of X directly.
 constexpr int kRhsG = 8;      // right-hand sides per pass
 constexpr int kFwdRows = 32;  // rows per CTA of k_fwd_large_rest
 
+// y_s = Li v_s by one CTA of 256 threads: thread (row i, half h) sums k in
+// [64h, 64h + 64) for a group of 8 right-hand sides (Li is zero above its
+// diagonal and outside w x w, so the loops have fixed trip counts and the
+// loads pipeline); halves meet in shared memory.  v is read past L1: other
+// CTAs wrote it.
 template <typename T>
-__global__ void k_fwd_large_gather(DevFronts F, const int32_t* list, const T* X, int64_t ldx, T* V, int nrhs) {
-  const int f = list[blockIdx.x];
-  const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
-  for (int r = 0; r < nrhs; ++r) {
-    T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
-    for (int i = threadIdx.x; i < nf; i += blockDim.x) Vf[i] = i < nc ? X[first + i + r * ldx] : T(0);
-    __syncthreads();
-    for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
-      const int c = F.child[t];
-      const int ncc = F.nc[c], nrc = F.nr[c];
-      const T* Vc = V + F.v_off[c] * nrhs + (int64_t)r * (ncc + nrc) + ncc;
-      const int32_t* loc = F.local + F.lrow_off[c];
-      for (int i = threadIdx.x; i < nrc; i += blockDim.x) Vf[loc[i] - 1] += Vc[i];
-      __syncthreads();
-    }
-  }
-}
-
-// y_s = Li v_s: thread (row i, half h) sums k in [64h, 64h + 64) for a group of
-// 8 right-hand sides (Li is zero above its diagonal and outside w x w, so the
-// loops have fixed trip counts and the loads pipeline); halves meet in shared memory
-template <typename T>
-__global__ void __launch_bounds__(256) k_fwd_large_diag(DevFronts F, const int32_t* list, int step,
-                                                        const T* __restrict__ dinv, T* X, int64_t ldx, T* V,
-                                                        int nrhs) {
-  __shared__ T vs[kSolveB * kRhsG];
-  __shared__ T hs[kSolveB * kRhsG];
-  const int f = list[blockIdx.x];
-  const int nc = F.nc[f], nf = nc + F.nr[f];
+__device__ void fwd_diag_cta(const DevFronts& F, int f, int step, int slot, const T* __restrict__ dinv, T* X,
+                             int64_t ldx, T* Vf, int nf, int nrhs, T* vs, T* hs) {
+  const int nc = F.nc[f];
   const int c0 = step * kSolveB;
-  if (c0 >= nc) return;
   const int w = min(kSolveB, nc - c0);
-  const T* Li = inv_block(F, dinv, f, step, blockIdx.x);
-  T* Vf = V + F.v_off[f] * nrhs;
+  const T* Li = inv_block(F, dinv, f, step, slot);
   const int first = F.first[f];
   const int tid = threadIdx.x, i = tid & (kSolveB - 1), h = tid >> 7;
   for (int r0 = 0; r0 < nrhs; r0 += kRhsG) {
@@ -1188,7 +1166,7 @@ __global__ void __launch_bounds__(256) k_fwd_large_diag(DevFronts F, const int32
     __syncthreads();
     for (int e = tid; e < kSolveB * kRhsG; e += blockDim.x) {
       const int k = e % kSolveB, r = e / kSolveB;
-      vs[k * kRhsG + r] = (k < w && r < g) ? Vf[(int64_t)(r0 + r) * nf + c0 + k] : T(0);
+      vs[k * kRhsG + r] = (k < w && r < g) ? __ldcg(&Vf[(int64_t)(r0 + r) * nf + c0 + k]) : T(0);
     }
     __syncthreads();
     T acc[kRhsG];
@@ -1219,19 +1197,53 @@ __global__ void __launch_bounds__(256) k_fwd_large_diag(DevFronts F, const int32
   }
 }
 
+// gather v (own X entries + the children's update vectors), then y_0
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwd_large_gather(DevFronts F, const int32_t* list,
+                                                          const T* __restrict__ dinv, T* X, int64_t ldx, T* V,
+                                                          int nrhs) {
+  __shared__ T vs[kSolveB * kRhsG];
+  __shared__ T hs[kSolveB * kRhsG];
+  const int f = list[blockIdx.x];
+  const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
+  T* Vbase = V + F.v_off[f] * nrhs;
+  for (int r = 0; r < nrhs; ++r) {
+    T* Vf = Vbase + (int64_t)r * nf;
+    for (int i = threadIdx.x; i < nf; i += blockDim.x) Vf[i] = i < nc ? X[first + i + r * ldx] : T(0);
+    __syncthreads();
+    for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
+      const int c = F.child[t];
+      const int ncc = F.nc[c], nrc = F.nr[c];
+      const T* Vc = V + F.v_off[c] * nrhs + (int64_t)r * (ncc + nrc) + ncc;
+      const int32_t* loc = F.local + F.lrow_off[c];
+      for (int i = threadIdx.x; i < nrc; i += blockDim.x) Vf[loc[i] - 1] += Vc[i];
+      __syncthreads();
+    }
+  }
+  __threadfence_block();
+  fwd_diag_cta(F, f, 0, blockIdx.x, dinv, X, ldx, Vbase, nf, nrhs, vs, hs);
+}
+
 // v_rest -= L_rest,s y_s: 32 rows per CTA (lane = row), warp q takes panel
-// columns 16q .. 16q+15 (held in registers), partial sums reduced in shared memory
+// columns 16q .. 16q+15 (held in registers), partial sums reduced in shared
+// memory; the front's last CTA then forms y_{s+1}
 template <typename T>
 __global__ void __launch_bounds__(256) k_fwd_large_rest(DevFronts F, const int32_t* list, int step,
-                                                        const T* __restrict__ panel, T* V, int nrhs) {
+                                                        const T* __restrict__ panel, const T* __restrict__ dinv,
+                                                        T* X, int64_t ldx, T* V, int32_t* cnt, int nrhs) {
   __shared__ T part[8][kRhsG][32];
+  __shared__ T vs[kSolveB * kRhsG];
+  __shared__ T hs[kSolveB * kRhsG];
+  __shared__ int last;
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int c0 = step * kSolveB;
   if (c0 >= nc) return;
   const int w = min(kSolveB, nc - c0);
-  const int rbase = c0 + w + blockIdx.x * kFwdRows;
+  const int rs0 = c0 + w;
+  const int rbase = rs0 + blockIdx.x * kFwdRows;
   if (rbase >= nf) return;
+  const int nchunks = (nf - rs0 + kFwdRows - 1) / kFwdRows;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int i = rbase + lane;
   const bool valid = i < nf;
@@ -1268,6 +1280,15 @@ __global__ void __launch_bounds__(256) k_fwd_large_rest(DevFronts F, const int32
     }
     __syncthreads();
   }
+  if (rs0 >= nc) return;                                 // no next step for this front
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&cnt[blockIdx.y], 1) == nchunks - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  fwd_diag_cta(F, f, step + 1, blockIdx.y, dinv, X, ldx, Vf, nf, nrhs, vs, hs);
+  if (threadIdx.x == 0) cnt[blockIdx.y] = 0;
 }
 
 template <typename T>
@@ -1756,16 +1777,15 @@ void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf
 }
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
-                      const T* dinv, T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st, int64_t* launches) {
+                      const T* dinv, T* X, int64_t ldx, T* V, int32_t* cnt, int nrhs, cudaStream_t st,
+                      int64_t* launches) {
   if (count <= 0) return;
-  k_fwd_large_gather<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
+  k_fwd_large_gather<T><<<count, 256, 0, st>>>(F, list, dinv, X, ldx, V, nrhs);
   const int steps = ceil_div(max_nc, kSolveB);
   const int chunks = std::max(1, ceil_div(max_nf, kFwdRows));
-  for (int s = 0; s < steps; ++s) {
-    k_fwd_large_diag<T><<<count, 256, 0, st>>>(F, list, s, dinv, X, ldx, V, nrhs);
-    k_fwd_large_rest<T><<<dim3(chunks, count), 256, 0, st>>>(F, list, s, panel, V, nrhs);
-  }
-  if (launches) *launches += 1 + 2 * steps;
+  for (int s = 0; s < steps; ++s)
+    k_fwd_large_rest<T><<<dim3(chunks, count), 256, 0, st>>>(F, list, s, panel, dinv, X, ldx, V, cnt, nrhs);
+  if (launches) *launches += 1 + steps;
 }
 template <typename T>
 void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
@@ -1834,7 +1854,7 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
   template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, int,         \
                                     cudaStream_t);                                                                 \
   template void launch_fwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
-                                    int64_t, T*, int, cudaStream_t, int64_t*);                                     \
+                                    int64_t, T*, int32_t*, int, cudaStream_t, int64_t*);                           \
   template void launch_bwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
                                     int64_t, T*, T*, int32_t*, int, cudaStream_t, int64_t*);                       \
   template void launch_permute_in<T>(const double*, int64_t, const int32_t*, T*, int64_t, int64_t, int,            \

@@ -127,7 +127,8 @@ void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf
 // Large fronts: dinv holds the inverted 128 x 128 diagonal blocks the factorization kept (DevFronts::d_off).
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
-                      const T* dinv, T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st, int64_t* launches);
+                      const T* dinv, T* X, int64_t ldx, T* V, int32_t* cnt, int nrhs, cudaStream_t st,
+                      int64_t* launches);
 // cnt: one zero-initialised ticket per list slot (left zero again on exit)
 template <typename T>
 void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,

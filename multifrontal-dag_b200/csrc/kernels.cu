@@ -1145,6 +1145,7 @@ __global__ void __launch_bounds__(kWFWarps * 32) k_bwd_small_warp(DevFronts F, c
 //             x_s = Li^T t_s (k_bwd_large_step)
 // The diagonal solves write the front's own entries of X directly.
 constexpr int kRhsG = 8;      // right-hand sides per pass
+constexpr int kMrhsMin = 8;   // from this many right-hand sides on, GEMM-shaped large-front steps
 constexpr int kFwdRows = 32;  // rows per CTA of k_fwd_large_rest
 
 // y_s = Li v_s by one CTA of 256 threads: thread (row i, half h) sums k in
@@ -1220,6 +1221,7 @@ __global__ void __launch_bounds__(256) k_fwd_large_gather(DevFronts F, const int
       __syncthreads();
     }
   }
+  if (nrhs >= kMrhsMin) return;          // the GEMM-shaped diagonal kernel follows
   __threadfence_block();
   fwd_diag_cta(F, f, 0, blockIdx.x, dinv, X, ldx, Vbase, nf, nrhs, vs, hs);
 }
@@ -1541,6 +1543,199 @@ __global__ void __launch_bounds__(256) k_bwd_large_step(DevFronts F, const int32
   if (nchunks > 0 && threadIdx.x == 0) cnt[blockIdx.y] = 0;
 }
 
+// ---- many right-hand sides (nrhs >= kMrhsMin): GEMM-shaped large-front steps --
+// V of a front is an nf x nrhs column-major block (ld nf).  Register-tiled
+// FMA GEMMs over 64-wide RHS tiles, operands staged through shared memory in
+// K chunks of 32:
+//   forward step s : Y = Li V_s        (k_mrhs_diag, transposed = false)
+//                    V_rest -= L_rest,s Y            (k_mrhs_fwd_rest)
+//   backward step s: partial(chunk) = L_chunk,s^T X_chunk   (k_mrhs_bwd_part)
+//                    X_s = Li^T (V_s - sum of partials)    (k_mrhs_diag, transposed = true)
+constexpr int kMT = 64;          // RHS tile
+constexpr int kMK = 32;          // K chunk
+
+// Y (128 x 64 RHS tile) = op(Li) V_s with op = identity or transpose; for the
+// backward step V_s is first reduced with the chunk partials.  Writes V_s and X.
+template <typename T>
+__global__ void __launch_bounds__(256) k_mrhs_diag(DevFronts F, const int32_t* list, int step,
+                                                   const T* __restrict__ dinv, T* X, int64_t ldx, T* V,
+                                                   const T* scratch, int nrhs, int transposed) {
+  constexpr int KC = 16;   // K chunk (128-row operand: keeps shared memory under 48 KB in FP64)
+  __shared__ T As[KC][kSolveB + 4];   // op(Li)(i, k) for the chunk, [k][i]
+  __shared__ T Bs[KC][kMT + 4];       // V_s(k, r)
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kSolveB;
+  if (c0 >= nc) return;
+  const int w = min(kSolveB, nc - c0);
+  const int r0 = blockIdx.x * kMT;
+  if (r0 >= nrhs) return;
+  const int rt = min(kMT, nrhs - r0);
+  const T* Li = inv_block(F, dinv, f, step, blockIdx.y);
+  T* Vf = V + F.v_off[f] * nrhs;
+  const int rs0 = c0 + w;
+  const int nchunks = (transposed && nf > rs0) ? (nf - rs0 + kSolveRows - 1) / kSolveRows : 0;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // rows ty + 16 m (8), RHS tx + 16 n (4)
+  T acc[8][4] = {};
+  for (int k0 = 0; k0 < w; k0 += KC) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < KC * kSolveB; e += blockDim.x) {
+      const int i = e % kSolveB, k = e / kSolveB;
+      T v = T(0);
+      if (k0 + k < w && i < w) v = transposed ? Li[(k0 + k) + (size_t)i * kSolveB] : Li[i + (size_t)(k0 + k) * kSolveB];
+      As[k][i] = v;
+    }
+    for (int e = threadIdx.x; e < KC * kMT; e += blockDim.x) {
+      const int k = e % KC, r = e / KC;
+      T v = T(0);
+      if (k0 + k < w && r < rt) {
+        const int64_t col = (int64_t)(r0 + r) * nf;
+        v = Vf[col + c0 + k0 + k];
+        for (int q = 0; q < nchunks; ++q)
+          v -= scratch[F.s_off[f] * nrhs + ((int64_t)(r0 + r) * nchunks + q) * kSolveB + k0 + k];
+      }
+      Bs[k][r] = v;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < KC; ++k) {
+      T a[8], b[4];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) a[m] = As[k][ty + 16 * m];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) b[n] = Bs[k][tx + 16 * n];
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+#pragma unroll
+        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * b[n];
+    }
+  }
+  __syncthreads();   // every CTA of this RHS tile read V_s before anyone overwrites it
+  const int first = F.first[f];
+#pragma unroll
+  for (int m = 0; m < 8; ++m)
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      const int i = ty + 16 * m, r = tx + 16 * n;
+      if (i < w && r < rt) {
+        Vf[(int64_t)(r0 + r) * nf + c0 + i] = acc[m][n];
+        X[first + c0 + i + (int64_t)(r0 + r) * ldx] = acc[m][n];
+      }
+    }
+}
+
+// V_rest(64-row tile, 64 RHS) -= L(rows, step columns) Y_s
+template <typename T>
+__global__ void __launch_bounds__(256) k_mrhs_fwd_rest(DevFronts F, const int32_t* list, int step,
+                                                       const T* __restrict__ panel, T* V, int nrhs) {
+  __shared__ T As[kMK][kMT + 4];       // L(row, k), [k][row]
+  __shared__ T Bs[kMK][kMT + 4];       // Y(k, r)
+  const int f = list[blockIdx.z];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kSolveB;
+  if (c0 >= nc) return;
+  const int w = min(kSolveB, nc - c0);
+  const int i0 = c0 + w + blockIdx.x * kMT;
+  if (i0 >= nf) return;
+  const int r0 = blockIdx.y * kMT;
+  if (r0 >= nrhs) return;
+  const int rt = min(kMT, nrhs - r0);
+  const T* P = panel + F.panel_off[f];
+  T* Vf = V + F.v_off[f] * nrhs;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // rows ty + 16 m (4), RHS tx + 16 n (4)
+  T acc[4][4] = {};
+  for (int k0 = 0; k0 < w; k0 += kMK) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < kMK * kMT; e += blockDim.x) {
+      const int i = e % kMT, k = e / kMT;
+      As[k][i] = (i0 + i < nf && k0 + k < w) ? P[(i0 + i) + (size_t)(c0 + k0 + k) * nf] : T(0);
+    }
+    for (int e = threadIdx.x; e < kMK * kMT; e += blockDim.x) {
+      const int k = e % kMK, r = e / kMK;
+      Bs[k][r] = (k0 + k < w && r < rt) ? Vf[(int64_t)(r0 + r) * nf + c0 + k0 + k] : T(0);
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < kMK; ++k) {
+      T a[4], b[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) a[m] = As[k][ty + 16 * m];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) b[n] = Bs[k][tx + 16 * n];
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * b[n];
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      const int i = i0 + ty + 16 * m, r = tx + 16 * n;
+      if (i < nf && r < rt) Vf[(int64_t)(r0 + r) * nf + i] -= acc[m][n];
+    }
+}
+
+// partial(chunk)(128 columns, 64 RHS) = L(chunk rows, step columns)^T X(chunk rows)
+template <typename T>
+__global__ void __launch_bounds__(256) k_mrhs_bwd_part(DevFronts F, const int32_t* list, int step,
+                                                       const T* __restrict__ panel, const T* V, T* scratch,
+                                                       int nrhs) {
+  constexpr int KC = 16;   // K chunk (128-row operand: keeps shared memory under 48 KB in FP64)
+  __shared__ T As[KC][kSolveB + 4];   // L(row, col), [row][col]
+  __shared__ T Bs[KC][kMT + 4];       // X(row, r)
+  const int f = list[blockIdx.z];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kSolveB;
+  if (c0 >= nc) return;
+  const int w = min(kSolveB, nc - c0);
+  const int rs0 = c0 + w;
+  const int rbase = rs0 + blockIdx.x * kSolveRows;
+  if (rbase >= nf) return;
+  const int nchunks = (nf - rs0 + kSolveRows - 1) / kSolveRows;
+  const int r0 = blockIdx.y * kMT;
+  if (r0 >= nrhs) return;
+  const int rt = min(kMT, nrhs - r0);
+  const int rend = min(nf, rbase + kSolveRows);
+  const T* P = panel + F.panel_off[f];
+  const T* Vf = V + F.v_off[f] * nrhs;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // columns ty + 16 m (8), RHS tx + 16 n (4)
+  T acc[8][4] = {};
+  for (int k0 = rbase; k0 < rend; k0 += KC) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < KC * kSolveB; e += blockDim.x) {
+      const int k = e % KC, col = e / KC;     // rows contiguous in global
+      As[k][col] = (k0 + k < rend && col < w) ? P[(k0 + k) + (size_t)(c0 + col) * nf] : T(0);
+    }
+    for (int e = threadIdx.x; e < KC * kMT; e += blockDim.x) {
+      const int k = e % KC, r = e / KC;
+      Bs[k][r] = (k0 + k < rend && r < rt) ? Vf[(int64_t)(r0 + r) * nf + k0 + k] : T(0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < KC; ++k) {
+      T a[8], b[4];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) a[m] = As[k][ty + 16 * m];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) b[n] = Bs[k][tx + 16 * n];
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+#pragma unroll
+        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * b[n];
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 8; ++m)
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      const int col = ty + 16 * m, r = tx + 16 * n;
+      if (col < w && r < rt)
+        scratch[F.s_off[f] * nrhs + ((int64_t)(r0 + r) * nchunks + blockIdx.x) * kSolveB + col] = acc[m][n];
+    }
+}
+
 // ============================================================================
 // vectors
 // ============================================================================
@@ -1782,6 +1977,15 @@ void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int ma
   if (count <= 0) return;
   k_fwd_large_gather<T><<<count, 256, 0, st>>>(F, list, dinv, X, ldx, V, nrhs);
   const int steps = ceil_div(max_nc, kSolveB);
+  if (nrhs >= kMrhsMin) {
+    const int rtiles = ceil_div(nrhs, kMT), rows = std::max(1, ceil_div(max_nf, kMT));
+    for (int s = 0; s < steps; ++s) {
+      k_mrhs_diag<T><<<dim3(rtiles, count), 256, 0, st>>>(F, list, s, dinv, X, ldx, V, nullptr, nrhs, 0);
+      k_mrhs_fwd_rest<T><<<dim3(rows, rtiles, count), 256, 0, st>>>(F, list, s, panel, V, nrhs);
+    }
+    if (launches) *launches += 1 + 2 * steps;
+    return;
+  }
   const int chunks = std::max(1, ceil_div(max_nf, kFwdRows));
   for (int s = 0; s < steps; ++s)
     k_fwd_large_rest<T><<<dim3(chunks, count), 256, 0, st>>>(F, list, s, panel, dinv, X, ldx, V, cnt, nrhs);
@@ -1795,6 +1999,15 @@ void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int ma
   k_bwd_large_gather<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
   const int steps = ceil_div(max_nc, kSolveB);
   const int chunks = std::max(1, ceil_div(max_nf, kSolveRows));
+  if (nrhs >= kMrhsMin) {
+    const int rtiles = ceil_div(nrhs, kMT);
+    for (int s = steps - 1; s >= 0; --s) {
+      k_mrhs_bwd_part<T><<<dim3(chunks, rtiles, count), 256, 0, st>>>(F, list, s, panel, V, scratch, nrhs);
+      k_mrhs_diag<T><<<dim3(rtiles, count), 256, 0, st>>>(F, list, s, dinv, X, ldx, V, scratch, nrhs, 1);
+    }
+    if (launches) *launches += 1 + 2 * steps;
+    return;
+  }
   for (int s = steps - 1; s >= 0; --s)
     k_bwd_large_step<T><<<dim3(chunks, count), 256, 0, st>>>(F, list, s, panel, dinv, X, ldx, V, scratch, cnt, nrhs);
   if (launches) *launches += 1 + steps;

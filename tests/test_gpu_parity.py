@@ -220,6 +220,25 @@ def test_multiple_rhs():
         assert np.abs(X[:, r] - xo).max() <= FP64_X_TOL * np.abs(xo).max()
 
 
+@pytest.mark.parametrize("nrhs", [8, 70])
+def test_many_rhs_large_fronts(nrhs):
+    """From 8 right-hand sides on, large fronts are solved with GEMM-shaped
+    steps (RHS tiles of 64: 70 spans two tiles); every column matches the
+    oracle's single-vector solve."""
+    p = P.laplace3d(16)
+    s = gpu_for(p, max_zero=1000)
+    o = oracle_for(p, max_zero=1000)
+    rng = np.random.default_rng(11)
+    B = np.asfortranarray(rng.uniform(-1, 1, (p.n, nrhs)))
+    X = B.copy(order="F")
+    rep, rc = s.solve(X)
+    assert rc == 0
+    for r in (0, nrhs // 2, nrhs - 1):
+        xo = o.solve(B[:, r])
+        assert np.abs(X[:, r] - xo).max() <= FP64_X_TOL * np.abs(xo).max(), r
+        assert P.backward_error(p.n, p.col, p.row, p.val, X[:, r], B[:, r]) <= FP64_BWD_TOL
+
+
 def test_deterministic_replay():
     p = P.laplace3d(12)
     s = gpu_for(p, small_front_max=40)

@@ -181,7 +181,7 @@ struct mfd_handle {
   void* d_panel = nullptr;
   void* d_upool = nullptr;
   void* d_diag = nullptr;
-  DBuf<double> d_a, d_b, d_xp, d_bp, d_r, d_norms;
+  DBuf<double> d_a, d_b, d_xp, d_bp, d_r, d_norms, d_cnorms;
   void* d_X = nullptr;   // T, n_total x nrhs
   void* d_V = nullptr;   // T
   void* d_S = nullptr;   // T
@@ -650,6 +650,7 @@ int ensure_rhs(mfd_handle* h, int nrhs) {
   CK(h->d_xp.alloc((size_t)h->n_total * nrhs));
   CK(h->d_bp.alloc((size_t)h->n_total * nrhs));
   CK(h->d_r.alloc((size_t)h->n_total * nrhs));
+  CK(h->d_cnorms.alloc((size_t)8 * nrhs));
   h->nrhs_cap = nrhs;
   return MFD_OK;
 }
@@ -1016,31 +1017,54 @@ int do_solve(mfd_handle* h, double* b, int nrhs, int64_t ldb, mfd_report* rep) {
     }
     launch_permute_out<double>(static_cast<double*>(h->d_X), n, h->d_perm.p, h->d_b.p, n, n, nrhs, st);
   } else {
-    // FP32 factor + FP64 iterative refinement, one right-hand side at a time
-    bool converged = true;
-    for (int r = 0; r < nrhs; ++r) {
-      double* bcol = h->d_b.p + (int64_t)r * n;
-      launch_permute_in<double>(bcol, n, h->d_perm.p, h->d_bp.p, n, n, 1, st);
-      CK(cudaMemsetAsync(h->d_xp.p, 0, sizeof(double) * n, st));
-      CK(cudaMemcpyAsync(h->d_r.p, h->d_bp.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-      int it = 0;
-      const int maxit = h->opt.ir_max_iter > 0 ? h->opt.ir_max_iter : 20;
-      double prev = 1e300;
-      for (; it < maxit; ++it) {
-        launch_to_t<float>(h->d_r.p, static_cast<float*>(h->d_X), n, st);
-        rc = solve_core<float>(h, 1);
-        if (rc) return rc;
-        launch_axpy_from_t<float>(static_cast<float*>(h->d_X), h->d_xp.p, n, st);
-        rc = residual_report(h, h->d_xp.p, h->d_bp.p, rep, &bwd);
-        if (rc) return rc;
-        if (bwd <= h->opt.ir_tol) { ++it; break; }
-        if (bwd > 0.9 * prev && it > 2) { ++it; break; }   // stagnation
-        prev = bwd;
+    // FP32 factor + FP64 iterative refinement, all right-hand sides together:
+    // one FP32 multi-RHS solve per sweep, FP64 residual and update per column,
+    // until every column's backward error is below the tolerance (or stagnates)
+    launch_permute_in<double>(h->d_b.p, n, h->d_perm.p, h->d_bp.p, n, n, nrhs, st);
+    CK(cudaMemsetAsync(h->d_xp.p, 0, sizeof(double) * n * nrhs, st));
+    CK(cudaMemcpyAsync(h->d_r.p, h->d_bp.p, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, st));
+    const int maxit = h->opt.ir_max_iter > 0 ? h->opt.ir_max_iter : 20;
+    std::vector<double> prev(nrhs, 1e300), cur(nrhs, 1e300), nv((size_t)8 * nrhs);
+    double worst_ref = 0;
+    int it = 0;
+    for (; it < maxit; ++it) {
+      launch_to_t<float>(h->d_r.p, static_cast<float*>(h->d_X), n * nrhs, st);
+      rc = solve_core<float>(h, nrhs);
+      if (rc) return rc;
+      launch_axpy_from_t<float>(static_cast<float*>(h->d_X), h->d_xp.p, n * nrhs, st);
+      for (int r = 0; r < nrhs; ++r) {
+        const int64_t o = (int64_t)r * n;
+        launch_residual(h->d_csr_ptr.p, h->d_csr_col.p, h->d_csr_val.p, h->d_xp.p + o, h->d_bp.p + o, h->d_r.p + o, n,
+                        st);
+        launch_norms(h->d_r.p + o, h->d_xp.p + o, h->d_bp.p + o, n, h->d_cnorms.p + 8 * r, st);
       }
-      iters = std::max(iters, it);
-      if (bwd > h->opt.ir_tol) converged = false;
-      launch_permute_out<double>(h->d_xp.p, n, h->d_perm.p, bcol, n, n, 1, st);
+      CK(cudaMemcpyAsync(nv.data(), h->d_cnorms.p, sizeof(double) * 8 * nrhs, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      bool all_ok = true, all_stalled = it > 2;
+      bwd = 0;
+      for (int r = 0; r < nrhs; ++r) {
+        const double* c = nv.data() + 8 * r;
+        const double denom = h->anorm * c[1] + c[2];
+        cur[r] = denom > 0 ? c[0] / denom : c[0];
+        if (cur[r] > h->opt.ir_tol) {
+          all_ok = false;
+          if (cur[r] <= 0.9 * prev[r]) all_stalled = false;
+        }
+        if (cur[r] >= bwd) {
+          bwd = cur[r];
+          worst_ref = c[4] > 0 ? std::sqrt(c[3]) / std::sqrt(c[4]) : std::sqrt(c[3]);
+        }
+        prev[r] = cur[r];
+      }
+      if (all_ok || all_stalled) { ++it; break; }
     }
+    iters = it;
+    const bool converged = bwd <= h->opt.ir_tol;
+    if (rep) {
+      rep->backward_error = bwd;
+      rep->residual_ref = worst_ref;
+    }
+    launch_permute_out<double>(h->d_xp.p, n, h->d_perm.p, h->d_b.p, n, n, nrhs, st);
     CK(cudaEventRecord(h->ev1, st));
     if (!converged) rc = MFD_E_NOCONV;
   }

@@ -306,6 +306,20 @@ def test_fp32_tensor_update_against_ffma(variant, tol):
     assert rc == 0 and rep.backward_error <= 1e-12
 
 
+def test_fp32_ir_many_rhs():
+    """Block refinement: all right-hand sides refined together, each column
+    to backward error <= 1e-12."""
+    p = P.laplace3d(16)
+    s = gpu_for(p, max_zero=1000, precision=H.MFD_PREC_FP32_IR)
+    rng = np.random.default_rng(5)
+    B = np.asfortranarray(rng.uniform(-1, 1, (p.n, 10)))
+    X = B.copy(order="F")
+    rep, rc = s.solve(X)
+    assert rc == 0 and rep.converged == 1
+    for r in range(10):
+        assert P.backward_error(p.n, p.col, p.row, p.val, X[:, r], B[:, r]) <= 1e-12, r
+
+
 # ---------------------------------------------------------------------------
 # batch of independent systems (uneven sizes)
 # ---------------------------------------------------------------------------

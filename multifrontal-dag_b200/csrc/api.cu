@@ -315,12 +315,20 @@ int build_plan(mfd_handle* h) {
     h->panel_elems += align_up((int64_t)nf * fr.nc);
     fr.v_off = h->v_elems;
     h->v_elems += nf;
-    fr.s_off = h->s_elems;
     fr.d_off = h->dinv_elems;
-    if (nf > sfm) {
-      h->s_elems += (int64_t)((nf + kSolveRows - 1) / kSolveRows) * kSolveB;
-      h->dinv_elems += (int64_t)((fr.nc + kFactB - 1) / kFactB) * kFactB * kFactB;   // kept for the solves
+    if (nf > sfm) h->dinv_elems += (int64_t)((fr.nc + kFactB - 1) / kFactB) * kFactB * kFactB;   // kept for the solves
+  }
+  // large-front solve partials: one region per level (levels solve one after
+  // another), kMrhsRows-row chunks cover the single-RHS 256-row chunks too
+  {
+    std::vector<int64_t> used(nlev, 0);
+    for (int32_t g = 0; g < nfr; ++g) {
+      HostFront& fr = h->fronts[g];
+      const int nf = fr.nc + fr.nr;
+      fr.s_off = used[fr.level];
+      if (nf > sfm) used[fr.level] += (int64_t)((nf + kMrhsRows - 1) / kMrhsRows) * kSolveB;
     }
+    for (int64_t u : used) h->s_elems = std::max(h->s_elems, u);
   }
   // update pool: static best-fit plan over level lifetimes
   {

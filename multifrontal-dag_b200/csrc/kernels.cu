@@ -1545,24 +1545,24 @@ __global__ void __launch_bounds__(256) k_bwd_large_step(DevFronts F, const int32
 
 // ---- many right-hand sides (nrhs >= kMrhsMin): GEMM-shaped large-front steps --
 // V of a front is an nf x nrhs column-major block (ld nf).  Register-tiled
-// FMA GEMMs over 64-wide RHS tiles, operands staged through shared memory in
-// K chunks of 32:
-//   forward step s : Y = Li V_s        (k_mrhs_diag, transposed = false)
-//                    V_rest -= L_rest,s Y            (k_mrhs_fwd_rest)
-//   backward step s: partial(chunk) = L_chunk,s^T X_chunk   (k_mrhs_bwd_part)
-//                    X_s = Li^T (V_s - sum of partials)    (k_mrhs_diag, transposed = true)
+// FMA GEMMs over 64-wide RHS tiles; operands stream through shared memory in
+// K chunks of 16 with cp.async double buffering (the next chunk's copies are
+// in flight while the current one is multiplied):
+//   forward step s : Y = Li V_s (k_mrhs_diag), V_rest -= L_rest,s Y (k_mrhs_fwd_rest)
+//   backward step s: partial(chunk) = L_chunk,s^T X_chunk (k_mrhs_bwd_part, 64-row chunks),
+//                    V_s -= sum of partials in chunk order (k_mrhs_bwd_reduce),
+//                    X_s = Li^T V_s (k_mrhs_diag, transposed)
 constexpr int kMT = 64;          // RHS tile
-constexpr int kMK = 32;          // K chunk
+constexpr int kMKc = 16;         // K chunk
 
-// Y (128 x 64 RHS tile) = op(Li) V_s with op = identity or transpose; for the
-// backward step V_s is first reduced with the chunk partials.  Writes V_s and X.
+// Y (128 x 64 RHS tile) = op(Li) V_s, op = identity or transpose; writes V_s and X
 template <typename T>
 __global__ void __launch_bounds__(256) k_mrhs_diag(DevFronts F, const int32_t* list, int step,
-                                                   const T* __restrict__ dinv, T* X, int64_t ldx, T* V,
-                                                   const T* scratch, int nrhs, int transposed) {
-  constexpr int KC = 16;   // K chunk (128-row operand: keeps shared memory under 48 KB in FP64)
-  __shared__ T As[KC][kSolveB + 4];   // op(Li)(i, k) for the chunk, [k][i]
-  __shared__ T Bs[KC][kMT + 4];       // V_s(k, r)
+                                                   const T* __restrict__ dinv, T* X, int64_t ldx, T* V, int nrhs,
+                                                   int transposed) {
+  constexpr int KC = sizeof(T) == 8 ? 8 : 16;   // K chunk: two 128-wide stages under 48 KB
+  __shared__ __align__(16) T As[2][KC][kSolveB + 4];   // op(Li)(i, k), [k][i]
+  __shared__ __align__(16) T Bs[2][KC][kMT + 4];       // V_s(k, r)
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int c0 = step * kSolveB;
@@ -1573,44 +1573,49 @@ __global__ void __launch_bounds__(256) k_mrhs_diag(DevFronts F, const int32_t* l
   const int rt = min(kMT, nrhs - r0);
   const T* Li = inv_block(F, dinv, f, step, blockIdx.y);
   T* Vf = V + F.v_off[f] * nrhs;
-  const int rs0 = c0 + w;
-  const int nchunks = (transposed && nf > rs0) ? (nf - rs0 + kSolveRows - 1) / kSolveRows : 0;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // rows ty + 16 m (8), RHS tx + 16 n (4)
-  T acc[8][4] = {};
-  for (int k0 = 0; k0 < w; k0 += KC) {
-    __syncthreads();
+  auto load = [&](int buf, int k0) {
     for (int e = threadIdx.x; e < KC * kSolveB; e += blockDim.x) {
-      const int i = e % kSolveB, k = e / kSolveB;
-      T v = T(0);
-      if (k0 + k < w && i < w) v = transposed ? Li[(k0 + k) + (size_t)i * kSolveB] : Li[i + (size_t)(k0 + k) * kSolveB];
-      As[k][i] = v;
+      int i, k;
+      if (transposed) { k = e % KC; i = e / KC; }   // Li(k0 + k, i): k contiguous in global
+      else { i = e % kSolveB; k = e / kSolveB; }         // Li(i, k0 + k): i contiguous
+      const bool v = k0 + k < w && i < w;
+      const T* src = transposed ? Li + (k0 + k) + (size_t)i * kSolveB : Li + i + (size_t)(k0 + k) * kSolveB;
+      cp_async_t(&As[buf][k][i], v ? src : Li, v);
     }
     for (int e = threadIdx.x; e < KC * kMT; e += blockDim.x) {
       const int k = e % KC, r = e / KC;
-      T v = T(0);
-      if (k0 + k < w && r < rt) {
-        const int64_t col = (int64_t)(r0 + r) * nf;
-        v = Vf[col + c0 + k0 + k];
-        for (int q = 0; q < nchunks; ++q)
-          v -= scratch[F.s_off[f] * nrhs + ((int64_t)(r0 + r) * nchunks + q) * kSolveB + k0 + k];
-      }
-      Bs[k][r] = v;
+      const bool v = k0 + k < w && r < rt;
+      cp_async_t(&Bs[buf][k][r], v ? Vf + (int64_t)(r0 + r) * nf + c0 + k0 + k : Vf, v);
+    }
+    cp_async_commit();
+  };
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // rows ty + 16 m (8), RHS tx + 16 n (4)
+  T acc[8][4] = {};
+  const int nch = (w + KC - 1) / KC;
+  load(0, 0);
+  for (int c = 0; c < nch; ++c) {
+    if (c + 1 < nch) {
+      load((c + 1) & 1, (c + 1) * KC);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
-#pragma unroll 4
+    const int b = c & 1;
+#pragma unroll
     for (int k = 0; k < KC; ++k) {
-      T a[8], b[4];
+      T a[8], bv[4];
 #pragma unroll
-      for (int m = 0; m < 8; ++m) a[m] = As[k][ty + 16 * m];
+      for (int m = 0; m < 8; ++m) a[m] = As[b][k][ty + 16 * m];
 #pragma unroll
-      for (int n = 0; n < 4; ++n) b[n] = Bs[k][tx + 16 * n];
+      for (int n = 0; n < 4; ++n) bv[n] = Bs[b][k][tx + 16 * n];
 #pragma unroll
       for (int m = 0; m < 8; ++m)
 #pragma unroll
-        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * b[n];
+        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * bv[n];
     }
+    __syncthreads();
   }
-  __syncthreads();   // every CTA of this RHS tile read V_s before anyone overwrites it
   const int first = F.first[f];
 #pragma unroll
   for (int m = 0; m < 8; ++m)
@@ -1628,8 +1633,8 @@ __global__ void __launch_bounds__(256) k_mrhs_diag(DevFronts F, const int32_t* l
 template <typename T>
 __global__ void __launch_bounds__(256) k_mrhs_fwd_rest(DevFronts F, const int32_t* list, int step,
                                                        const T* __restrict__ panel, T* V, int nrhs) {
-  __shared__ T As[kMK][kMT + 4];       // L(row, k), [k][row]
-  __shared__ T Bs[kMK][kMT + 4];       // Y(k, r)
+  __shared__ __align__(16) T As[2][kMKc][kMT + 4];   // L(row, k), [k][row]
+  __shared__ __align__(16) T Bs[2][kMKc][kMT + 4];   // Y(k, r)
   const int f = list[blockIdx.z];
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int c0 = step * kSolveB;
@@ -1642,31 +1647,45 @@ __global__ void __launch_bounds__(256) k_mrhs_fwd_rest(DevFronts F, const int32_
   const int rt = min(kMT, nrhs - r0);
   const T* P = panel + F.panel_off[f];
   T* Vf = V + F.v_off[f] * nrhs;
+  auto load = [&](int buf, int k0) {
+    for (int e = threadIdx.x; e < kMKc * kMT; e += blockDim.x) {
+      const int i = e % kMT, k = e / kMT;
+      const bool v = i0 + i < nf && k0 + k < w;
+      cp_async_t(&As[buf][k][i], v ? P + (i0 + i) + (size_t)(c0 + k0 + k) * nf : P, v);
+    }
+    for (int e = threadIdx.x; e < kMKc * kMT; e += blockDim.x) {
+      const int k = e % kMKc, r = e / kMKc;
+      const bool v = k0 + k < w && r < rt;
+      cp_async_t(&Bs[buf][k][r], v ? Vf + (int64_t)(r0 + r) * nf + c0 + k0 + k : Vf, v);
+    }
+    cp_async_commit();
+  };
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // rows ty + 16 m (4), RHS tx + 16 n (4)
   T acc[4][4] = {};
-  for (int k0 = 0; k0 < w; k0 += kMK) {
-    __syncthreads();
-    for (int e = threadIdx.x; e < kMK * kMT; e += blockDim.x) {
-      const int i = e % kMT, k = e / kMT;
-      As[k][i] = (i0 + i < nf && k0 + k < w) ? P[(i0 + i) + (size_t)(c0 + k0 + k) * nf] : T(0);
+  const int nch = (w + kMKc - 1) / kMKc;
+  load(0, 0);
+  for (int c = 0; c < nch; ++c) {
+    if (c + 1 < nch) {
+      load((c + 1) & 1, (c + 1) * kMKc);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
-    for (int e = threadIdx.x; e < kMK * kMT; e += blockDim.x) {
-      const int k = e % kMK, r = e / kMK;
-      Bs[k][r] = (k0 + k < w && r < rt) ? Vf[(int64_t)(r0 + r) * nf + c0 + k0 + k] : T(0);
-    }
     __syncthreads();
-#pragma unroll 8
-    for (int k = 0; k < kMK; ++k) {
-      T a[4], b[4];
+    const int b = c & 1;
 #pragma unroll
-      for (int m = 0; m < 4; ++m) a[m] = As[k][ty + 16 * m];
+    for (int k = 0; k < kMKc; ++k) {
+      T a[4], bv[4];
 #pragma unroll
-      for (int n = 0; n < 4; ++n) b[n] = Bs[k][tx + 16 * n];
+      for (int m = 0; m < 4; ++m) a[m] = As[b][k][ty + 16 * m];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) bv[n] = Bs[b][k][tx + 16 * n];
 #pragma unroll
       for (int m = 0; m < 4; ++m)
 #pragma unroll
-        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * b[n];
+        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * bv[n];
     }
+    __syncthreads();
   }
 #pragma unroll
   for (int m = 0; m < 4; ++m)
@@ -1677,54 +1696,68 @@ __global__ void __launch_bounds__(256) k_mrhs_fwd_rest(DevFronts F, const int32_
     }
 }
 
-// partial(chunk)(128 columns, 64 RHS) = L(chunk rows, step columns)^T X(chunk rows)
+// partial(chunk)(128 columns, 64 RHS) = L(chunk rows, step columns)^T X(chunk rows), 64-row chunks
 template <typename T>
 __global__ void __launch_bounds__(256) k_mrhs_bwd_part(DevFronts F, const int32_t* list, int step,
                                                        const T* __restrict__ panel, const T* V, T* scratch,
                                                        int nrhs) {
-  constexpr int KC = 16;   // K chunk (128-row operand: keeps shared memory under 48 KB in FP64)
-  __shared__ T As[KC][kSolveB + 4];   // L(row, col), [row][col]
-  __shared__ T Bs[KC][kMT + 4];       // X(row, r)
+  constexpr int KC = sizeof(T) == 8 ? 8 : 16;   // K chunk: two 128-wide stages under 48 KB
+  __shared__ __align__(16) T As[2][KC][kSolveB + 4];   // L(row, col), [row][col]
+  __shared__ __align__(16) T Bs[2][KC][kMT + 4];       // X(row, r)
   const int f = list[blockIdx.z];
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int c0 = step * kSolveB;
   if (c0 >= nc) return;
   const int w = min(kSolveB, nc - c0);
   const int rs0 = c0 + w;
-  const int rbase = rs0 + blockIdx.x * kSolveRows;
+  const int rbase = rs0 + blockIdx.x * kMrhsRows;
   if (rbase >= nf) return;
-  const int nchunks = (nf - rs0 + kSolveRows - 1) / kSolveRows;
+  const int nchunks = (nf - rs0 + kMrhsRows - 1) / kMrhsRows;
   const int r0 = blockIdx.y * kMT;
   if (r0 >= nrhs) return;
   const int rt = min(kMT, nrhs - r0);
-  const int rend = min(nf, rbase + kSolveRows);
+  const int rend = min(nf, rbase + kMrhsRows);
   const T* P = panel + F.panel_off[f];
   const T* Vf = V + F.v_off[f] * nrhs;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // columns ty + 16 m (8), RHS tx + 16 n (4)
-  T acc[8][4] = {};
-  for (int k0 = rbase; k0 < rend; k0 += KC) {
-    __syncthreads();
+  auto load = [&](int buf, int k0) {
     for (int e = threadIdx.x; e < KC * kSolveB; e += blockDim.x) {
       const int k = e % KC, col = e / KC;     // rows contiguous in global
-      As[k][col] = (k0 + k < rend && col < w) ? P[(k0 + k) + (size_t)(c0 + col) * nf] : T(0);
+      const bool v = k0 + k < rend && col < w;
+      cp_async_t(&As[buf][k][col], v ? P + (k0 + k) + (size_t)(c0 + col) * nf : P, v);
     }
     for (int e = threadIdx.x; e < KC * kMT; e += blockDim.x) {
       const int k = e % KC, r = e / KC;
-      Bs[k][r] = (k0 + k < rend && r < rt) ? Vf[(int64_t)(r0 + r) * nf + k0 + k] : T(0);
+      const bool v = k0 + k < rend && r < rt;
+      cp_async_t(&Bs[buf][k][r], v ? Vf + (int64_t)(r0 + r) * nf + k0 + k : Vf, v);
+    }
+    cp_async_commit();
+  };
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // columns ty + 16 m (8), RHS tx + 16 n (4)
+  T acc[8][4] = {};
+  const int nch = (rend - rbase + KC - 1) / KC;
+  load(0, rbase);
+  for (int c = 0; c < nch; ++c) {
+    if (c + 1 < nch) {
+      load((c + 1) & 1, rbase + (c + 1) * KC);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
-#pragma unroll 4
+    const int b = c & 1;
+#pragma unroll
     for (int k = 0; k < KC; ++k) {
-      T a[8], b[4];
+      T a[8], bv[4];
 #pragma unroll
-      for (int m = 0; m < 8; ++m) a[m] = As[k][ty + 16 * m];
+      for (int m = 0; m < 8; ++m) a[m] = As[b][k][ty + 16 * m];
 #pragma unroll
-      for (int n = 0; n < 4; ++n) b[n] = Bs[k][tx + 16 * n];
+      for (int n = 0; n < 4; ++n) bv[n] = Bs[b][k][tx + 16 * n];
 #pragma unroll
       for (int m = 0; m < 8; ++m)
 #pragma unroll
-        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * b[n];
+        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * bv[n];
     }
+    __syncthreads();
   }
 #pragma unroll
   for (int m = 0; m < 8; ++m)
@@ -1734,6 +1767,25 @@ __global__ void __launch_bounds__(256) k_mrhs_bwd_part(DevFronts F, const int32_
       if (col < w && r < rt)
         scratch[F.s_off[f] * nrhs + ((int64_t)(r0 + r) * nchunks + blockIdx.x) * kSolveB + col] = acc[m][n];
     }
+}
+
+// V_s(k, r) -= sum over chunks of partial (chunk order), one thread per entry
+template <typename T>
+__global__ void __launch_bounds__(256) k_mrhs_bwd_reduce(DevFronts F, const int32_t* list, int step, T* V,
+                                                         const T* scratch, int nrhs) {
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int c0 = step * kSolveB;
+  if (c0 >= nc) return;
+  const int w = min(kSolveB, nc - c0);
+  const int rs0 = c0 + w;
+  const int nchunks = nf > rs0 ? (nf - rs0 + kMrhsRows - 1) / kMrhsRows : 0;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = e % kSolveB, r = e / kSolveB;
+  if (nchunks == 0 || r >= nrhs || k >= w) return;
+  T s = V[F.v_off[f] * nrhs + (int64_t)r * nf + c0 + k];
+  for (int q = 0; q < nchunks; ++q) s -= scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + q) * kSolveB + k];
+  V[F.v_off[f] * nrhs + (int64_t)r * nf + c0 + k] = s;
 }
 
 // ============================================================================
@@ -1980,7 +2032,7 @@ void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int ma
   if (nrhs >= kMrhsMin) {
     const int rtiles = ceil_div(nrhs, kMT), rows = std::max(1, ceil_div(max_nf, kMT));
     for (int s = 0; s < steps; ++s) {
-      k_mrhs_diag<T><<<dim3(rtiles, count), 256, 0, st>>>(F, list, s, dinv, X, ldx, V, nullptr, nrhs, 0);
+      k_mrhs_diag<T><<<dim3(rtiles, count), 256, 0, st>>>(F, list, s, dinv, X, ldx, V, nrhs, 0);
       k_mrhs_fwd_rest<T><<<dim3(rows, rtiles, count), 256, 0, st>>>(F, list, s, panel, V, nrhs);
     }
     if (launches) *launches += 1 + 2 * steps;
@@ -2002,10 +2054,13 @@ void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int ma
   if (nrhs >= kMrhsMin) {
     const int rtiles = ceil_div(nrhs, kMT);
     for (int s = steps - 1; s >= 0; --s) {
-      k_mrhs_bwd_part<T><<<dim3(chunks, rtiles, count), 256, 0, st>>>(F, list, s, panel, V, scratch, nrhs);
-      k_mrhs_diag<T><<<dim3(rtiles, count), 256, 0, st>>>(F, list, s, dinv, X, ldx, V, scratch, nrhs, 1);
+      k_mrhs_bwd_part<T><<<dim3(std::max(1, ceil_div(max_nf, kMrhsRows)), rtiles, count), 256, 0, st>>>(
+          F, list, s, panel, V, scratch, nrhs);
+      k_mrhs_bwd_reduce<T><<<dim3(ceil_div((int64_t)kSolveB * nrhs, 256), count), 256, 0, st>>>(F, list, s, V, scratch,
+                                                                                                nrhs);
+      k_mrhs_diag<T><<<dim3(rtiles, count), 256, 0, st>>>(F, list, s, dinv, X, ldx, V, nrhs, 1);
     }
-    if (launches) *launches += 1 + 2 * steps;
+    if (launches) *launches += 1 + 3 * steps;
     return;
   }
   for (int s = steps - 1; s >= 0; --s)

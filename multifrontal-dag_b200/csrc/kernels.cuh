@@ -17,6 +17,7 @@ constexpr int kUpdTile = 128;        // trailing-update output tile (tensor path
 constexpr int kUpdTileSimt = 64;     // trailing-update output tile (FMA path)
 constexpr int kSolveB = kFactB;      // column step of the large-front solves (one inverted diagonal block)
 constexpr int kSolveRows = 256;      // rows per CTA of the backward large-front partial sums
+constexpr int kMrhsRows = 64;        // rows per CTA of the many-RHS backward partial sums
 
 #ifdef __CUDACC__
 // Lower tile (ti, tj) of the trailing T x T tile grid (tile width tw) handled by

@@ -899,7 +899,8 @@ __global__ void __launch_bounds__(256) k_fwd_small(DevFronts F, const int32_t* l
   for (int j = warp; j < nc; j += nw)
     for (int i = j + lane; i < nf; i += 32) L[i + j * ld] = P[i + (size_t)j * nf];
   const int first = F.first[f];
-  for (int r = 0; r < nrhs; ++r) {
+  const int rb = gridDim.y > 1 ? (int)blockIdx.y : 0, re = gridDim.y > 1 ? rb + 1 : nrhs;   // one RHS per CTA row
+  for (int r = rb; r < re; ++r) {
     __syncthreads();
     for (int i = tid; i < nf; i += nt) v[i] = i < nc ? X[first + i + r * ldx] : T(0);
     __syncthreads();
@@ -941,7 +942,8 @@ __global__ void __launch_bounds__(256) k_bwd_small(DevFronts F, const int32_t* l
     for (int i = j + lane; i < nf; i += 32) L[i + j * ld] = P[i + (size_t)j * nf];
   const int first = F.first[f];
   const int32_t* lr = F.lrow + F.lrow_off[f];
-  for (int r = 0; r < nrhs; ++r) {
+  const int rb = gridDim.y > 1 ? (int)blockIdx.y : 0, re = gridDim.y > 1 ? rb + 1 : nrhs;   // one RHS per CTA row
+  for (int r = rb; r < re; ++r) {
     __syncthreads();
     for (int i = tid; i < nf; i += nt) v[i] = i < nc ? X[first + i + r * ldx] : X[lr[i - nc] + r * ldx];
     __syncthreads();
@@ -1208,7 +1210,9 @@ __global__ void __launch_bounds__(256) k_fwd_large_gather(DevFronts F, const int
   const int f = list[blockIdx.x];
   const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
   T* Vbase = V + F.v_off[f] * nrhs;
-  for (int r = 0; r < nrhs; ++r) {
+  // one right-hand side per CTA when the grid has a y extent (many RHS)
+  const int rb = gridDim.y > 1 ? (int)blockIdx.y : 0, re = gridDim.y > 1 ? rb + 1 : nrhs;
+  for (int r = rb; r < re; ++r) {
     T* Vf = Vbase + (int64_t)r * nf;
     for (int i = threadIdx.x; i < nf; i += blockDim.x) Vf[i] = i < nc ? X[first + i + r * ldx] : T(0);
     __syncthreads();
@@ -1221,7 +1225,7 @@ __global__ void __launch_bounds__(256) k_fwd_large_gather(DevFronts F, const int
       __syncthreads();
     }
   }
-  if (nrhs >= kMrhsMin) return;          // the GEMM-shaped diagonal kernel follows
+  if (nrhs >= kMrhsMin || gridDim.y > 1) return;   // the GEMM-shaped diagonal kernel follows
   __threadfence_block();
   fwd_diag_cta(F, f, 0, blockIdx.x, dinv, X, ldx, Vbase, nf, nrhs, vs, hs);
 }
@@ -1298,7 +1302,8 @@ __global__ void k_bwd_large_gather(DevFronts F, const int32_t* list, const T* X,
   const int f = list[blockIdx.x];
   const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
   const int32_t* lr = F.lrow + F.lrow_off[f];
-  for (int r = 0; r < nrhs; ++r) {
+  const int rb = gridDim.y > 1 ? (int)blockIdx.y : 0, re = gridDim.y > 1 ? rb + 1 : nrhs;
+  for (int r = rb; r < re; ++r) {
     T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
     for (int i = threadIdx.x; i < nf; i += blockDim.x) Vf[i] = i < nc ? X[first + i + r * ldx] : X[lr[i - nc] + r * ldx];
   }
@@ -2008,7 +2013,7 @@ void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf
   }
   size_t sm = fwd_small_smem<T>(nf_max);
   set_smem(k_fwd_small<T>, sm);
-  k_fwd_small<T><<<count, 256, sm, st>>>(F, list, panel, X, ldx, V, nrhs);
+  k_fwd_small<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, sm, st>>>(F, list, panel, X, ldx, V, nrhs);
 }
 template <typename T>
 void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
@@ -2020,14 +2025,14 @@ void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf
   }
   size_t sm = fwd_small_smem<T>(nf_max);
   set_smem(k_bwd_small<T>, sm);
-  k_bwd_small<T><<<count, 256, sm, st>>>(F, list, panel, X, ldx, nrhs);
+  k_bwd_small<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, sm, st>>>(F, list, panel, X, ldx, nrhs);
 }
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
                       const T* dinv, T* X, int64_t ldx, T* V, int32_t* cnt, int nrhs, cudaStream_t st,
                       int64_t* launches) {
   if (count <= 0) return;
-  k_fwd_large_gather<T><<<count, 256, 0, st>>>(F, list, dinv, X, ldx, V, nrhs);
+  k_fwd_large_gather<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, 0, st>>>(F, list, dinv, X, ldx, V, nrhs);
   const int steps = ceil_div(max_nc, kSolveB);
   if (nrhs >= kMrhsMin) {
     const int rtiles = ceil_div(nrhs, kMT), rows = std::max(1, ceil_div(max_nf, kMT));
@@ -2048,7 +2053,7 @@ void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int ma
                       const T* dinv, T* X, int64_t ldx, T* V, T* scratch, int32_t* cnt, int nrhs, cudaStream_t st,
                       int64_t* launches) {
   if (count <= 0) return;
-  k_bwd_large_gather<T><<<count, 256, 0, st>>>(F, list, X, ldx, V, nrhs);
+  k_bwd_large_gather<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, 0, st>>>(F, list, X, ldx, V, nrhs);
   const int steps = ceil_div(max_nc, kSolveB);
   const int chunks = std::max(1, ceil_div(max_nf, kSolveRows));
   if (nrhs >= kMrhsMin) {

@@ -607,14 +607,16 @@ __device__ __forceinline__ T* trailing_addr(T* P, T* U, int nc, int nr, int nf, 
 
 // Trailing update on the FP64 tensor pipe: one 128x128 tile of the trailing
 // lower triangle per CTA, C -= P_i P_j^T over K = w <= 128 in chunks of 32,
-// double-buffered with cp.async.  8 warps as 2 (rows) x 4 (columns) of 64x32,
-// each 4 x 4 mma.m16n8k16.f64 per K step of 16.  Shared-memory operands are
+// double-buffered with cp.async.  16 warps as 4 (rows) x 4 (columns) of 32x32,
+// each 2 x 4 mma.m16n8k16.f64 per K step of 16.  Shared-memory operands are
 // k-major with a row stride of 132 doubles (= 4 mod 16): every fragment load of
 // a half-warp hits 16 distinct 8-byte bank pairs.  The accumulators are loaded
 // with C itself (8 rows x 4 column pairs per warp access: full 32-byte
 // sectors) while the first operand chunk is in flight, the A fragments enter
 // negated, and the epilogue only stores.
 constexpr int kUT = 128, kUK = 32, kULD = 132;
+constexpr int kUThreads = 512;              // 16 warps: 4 (rows) x 4 (columns) of 32 x 32
+constexpr int kUMF = kUT / (kUThreads / 32 / 4) / 16;   // m16 fragments per warp (2)
 
 __device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
   asm volatile(
@@ -720,7 +722,7 @@ __global__ void __launch_bounds__(256) k_trsm2(DevFronts F, const int32_t* list,
   }
 }
 
-__global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32_t* list, int step, double* panel,
+__global__ void __launch_bounds__(kUThreads, 1) k_update_dmma(DevFronts F, const int32_t* list, int step, double* panel,
                                                         double* upool, int mode) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* sm = reinterpret_cast<double*>(smem_raw);     // [stage][operand][k][row]
@@ -758,14 +760,14 @@ __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32
   const int g = lane >> 2, q = lane & 3;
   // the accumulators start as C (loads in flight with the first operand chunk) and the
   // A fragments enter negated, so the tile ends as C - P_i P_j^T and the epilogue only stores
-  const int rbase = i0 + wm * 64 + g, cbase = j0 + wn * 32 + 2 * q;
+  const int rbase = i0 + wm * (16 * kUMF) + g, cbase = j0 + wn * 32 + 2 * q;
   // C may be written by a kernel this one waits on through an event (the
   // lookahead's side stream): everything is read after the wait
   pdl_wait();
   pdl_trigger();
-  double acc[4][4][4];
+  double acc[kUMF][4][4];
 #pragma unroll
-  for (int mi = 0; mi < 4; ++mi)
+  for (int mi = 0; mi < kUMF; ++mi)
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
@@ -792,10 +794,10 @@ __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32
 #pragma unroll
         for (int i = 0; i < 4; ++i) bv[ni][i] = Bs[(kk + q + 4 * i) * kULD + wn * 32 + ni * 8 + g];
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi) {
+      for (int mi = 0; mi < kUMF; ++mi) {
         double av[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) av[i] = -As[(kk + q + 4 * (i >> 1)) * kULD + wm * 64 + mi * 16 + g + 8 * (i & 1)];
+        for (int i = 0; i < 8; ++i) av[i] = -As[(kk + q + 4 * (i >> 1)) * kULD + wm * (16 * kUMF) + mi * 16 + g + 8 * (i & 1)];
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) dmma16(acc[mi][ni], av, bv[ni]);
       }
@@ -803,7 +805,7 @@ __global__ void __launch_bounds__(256, 1) k_update_dmma(DevFronts F, const int32
     __syncthreads();
   }
 #pragma unroll
-  for (int mi = 0; mi < 4; ++mi)
+  for (int mi = 0; mi < kUMF; ++mi)
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
@@ -1992,7 +1994,7 @@ void launch_update(const DevFronts& F, const int32_t* list, int count, int step,
       const int g = update_grid(tiles128, kUT, mode);
       if (g <= 0) return;
       size_t sm = 2 * 2 * (size_t)kUK * kULD * sizeof(double);
-      launch_k(k_update_dmma, dim3(g, count), dim3(256), sm, st, pdl, F, list, step, reinterpret_cast<double*>(panel),
+      launch_k(k_update_dmma, dim3(g, count), dim3(kUThreads), sm, st, pdl, F, list, step, reinterpret_cast<double*>(panel),
                reinterpret_cast<double*>(upool), mode);
       return;
     }

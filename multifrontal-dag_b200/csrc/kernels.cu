@@ -37,6 +37,13 @@ __device__ __forceinline__ double dev_sqrt<double>(double x) { return sqrt(x); }
 template <>
 __device__ __forceinline__ float dev_sqrt<float>(float x) { return sqrtf(x); }
 
+template <typename T>
+__device__ __forceinline__ T rsqrt_t(T x);
+template <>
+__device__ __forceinline__ double rsqrt_t<double>(double x) { return rsqrt(x); }
+template <>
+__device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
+
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc, bool valid) {
@@ -57,6 +64,37 @@ __device__ __forceinline__ void cp_async_t(T* dst, const T* src, bool valid) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src), "r"(sz));
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(src), "r"(sz));
+}
+
+// Extend-add of one child's lower update triangle into a front held in shared
+// memory (ld ldS), by `nthreads` threads starting at index t0: each thread
+// gathers kEABatch entries (value and target, loads all in flight) before its
+// shared-memory adds.  local_index is injective, so no two entries of one
+// child share a target.
+constexpr int kEABatch = 8;
+// Packed lower storage (ldS < 0, nf = -ldS): column j starts at
+// j nf - j (j + 1) / 2 and holds rows j .. nf-1.
+__device__ __forceinline__ int packed_col(int j, int nf) { return j * nf - j * (j + 1) / 2; }
+
+template <typename T>
+__device__ __forceinline__ void extend_add_smem(T* S, int ldS, const T* __restrict__ U,
+                                                const int32_t* __restrict__ loc, int nrc, int t0, int nthreads) {
+  const int tot = nrc * nrc;
+  for (int e0 = t0; e0 < tot; e0 += nthreads * kEABatch) {
+    T val[kEABatch];
+    int dst[kEABatch];
+#pragma unroll
+    for (int u = 0; u < kEABatch; ++u) {
+      const int e = e0 + u * nthreads;
+      const int j = e / nrc, i = e - j * nrc;
+      const bool v = e < tot && i >= j;
+      val[u] = v ? U[i + (size_t)j * nrc] : T(0);
+      dst[u] = v ? (ldS > 0 ? (loc[i] - 1) + (loc[j] - 1) * ldS : packed_col(loc[j] - 1, -ldS) + (loc[i] - 1)) : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < kEABatch; ++u)
+      if (dst[u] >= 0) S[dst[u]] += val[u];
+  }
 }
 
 // Strided element loop (e = threadIdx.x, += blockDim.x, e < total) whose
@@ -200,57 +238,63 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_small_front(DevFronts F, const int32_t* list, const double* __restrict__ a,
                                                      T* __restrict__ panel, T* __restrict__ upool, int32_t* info) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* S = reinterpret_cast<T*>(smem_raw);
+  T* S = reinterpret_cast<T*>(smem_raw);     // the front's lower triangle, packed by columns
   const int f = list[blockIdx.x];
   const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
-  const int ld = nf | 1;
+  const int tri = nf * (nf + 1) / 2;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
 
-  for (int i = tid; i < ld * nf; i += nt) S[i] = T(0);
+  for (int i = tid; i < tri; i += nt) S[i] = T(0);
   __syncthreads();
   for (int k = F.a_beg[f] + tid; k < F.a_beg[f + 1]; k += nt) {
-    int pos = F.a_pos[k];
-    int c = pos / nf, r = pos - c * nf;
-    S[r + c * ld] = T(a[F.a_src[k]]);
+    const int pos = F.a_pos[k];
+    const int c = pos / nf, r = pos - c * nf;          // r >= c: the lower part of A
+    S[packed_col(c, nf) + r] = T(a[F.a_src[k]]);
   }
   __syncthreads();
   for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
     const int c = F.child[t];
-    const int nrc = F.nr[c];
-    const T* __restrict__ U = upool + F.u_off[c];
-    const int32_t* __restrict__ loc = F.local + F.lrow_off[c];
-    for (int j = warp; j < nrc; j += nw) {
-      const int lj = (loc[j] - 1) * ld;
-      const T* col = U + (size_t)j * nrc;
-      for (int i = j + lane; i < nrc; i += 32) S[(loc[i] - 1) + lj] += col[i];
+    extend_add_smem(S, -nf, upool + F.u_off[c], F.local + F.lrow_off[c], F.nr[c], tid, nt);
+    __syncthreads();
+  }
+  // unscaled right-looking elimination, two barriers per pivot: thread 0 forms
+  // y_k = 1/sqrt(d_k); then the trailing part takes -c_i c_j y_k^2 from the
+  // still unscaled column k while column k-1 is scaled to L(:, k-1)
+  T* ys = S + tri;                           // two pivot scales after the front
+  for (int k = 0; k < nc; ++k) {
+    T* colk = S + packed_col(k, nf);
+    if (tid == 0) {
+      T d = colk[k];
+      if (!(d > T(0))) { atomicMin(info, F.first[f] + k + 1); d = T(1); colk[k] = d; }
+      ys[k & 1] = rsqrt_t<T>(d);
+    }
+    __syncthreads();
+    const T y = ys[k & 1], y2 = y * y;
+    for (int j = k + 1 + warp; j < nf; j += nw) {
+      const T cj = colk[j] * y2;
+      T* colj = S + packed_col(j, nf);
+      for (int i = j + lane; i < nf; i += 32) colj[i] -= colk[i] * cj;
+    }
+    if (k > 0) {
+      T* colp = S + packed_col(k - 1, nf);
+      const T yp = ys[(k - 1) & 1];
+      for (int i = k - 1 + tid; i < nf; i += nt) colp[i] *= yp;      // diagonal: d y = sqrt(d)
     }
     __syncthreads();
   }
-  for (int k = 0; k < nc; ++k) {
-    T* colk = S + k * ld;
-    if (tid == 0) {
-      T d = colk[k];
-      if (!(d > T(0))) { atomicMin(info, F.first[f] + k + 1); d = T(1); }
-      colk[k] = dev_sqrt<T>(d);
-    }
-    __syncthreads();
-    const T inv = T(1) / colk[k];
-    for (int i = k + 1 + tid; i < nf; i += nt) colk[i] *= inv;
-    __syncthreads();
-    for (int j = k + 1 + warp; j < nf; j += nw) {
-      const T ljk = colk[j];
-      T* colj = S + j * ld;
-      for (int i = j + lane; i < nf; i += 32) colj[i] -= colk[i] * ljk;
-    }
+  if (nc > 0) {
+    T* colp = S + packed_col(nc - 1, nf);
+    const T yp = ys[(nc - 1) & 1];
+    for (int i = nc - 1 + tid; i < nf; i += nt) colp[i] *= yp;
     __syncthreads();
   }
   T* P = panel + F.panel_off[f];
   for (int j = warp; j < nc; j += nw)
-    for (int i = j + lane; i < nf; i += 32) P[i + (size_t)j * nf] = S[i + j * ld];
+    for (int i = j + lane; i < nf; i += 32) P[i + (size_t)j * nf] = S[packed_col(j, nf) + i];
   T* U = upool + F.u_off[f];
   for (int j = warp; j < nr; j += nw)
-    for (int i = j + lane; i < nr; i += 32) U[i + (size_t)j * nr] = S[(nc + i) + (nc + j) * ld];
+    for (int i = j + lane; i < nr; i += 32) U[i + (size_t)j * nr] = S[packed_col(nc + j, nf) + nc + i];
 }
 
 // Zero the lower triangles of a large front's panel (nf x nc) and update
@@ -978,12 +1022,6 @@ constexpr int kWF = 32;          // front capacity of a warp
 constexpr int kWFLd = kWF + 1;
 constexpr int kWFWarps = 4;
 
-template <typename T>
-__device__ __forceinline__ T rsqrt_t(T x);
-template <>
-__device__ __forceinline__ double rsqrt_t<double>(double x) { return rsqrt(x); }
-template <>
-__device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
 
 template <typename T>
 __global__ void __launch_bounds__(kWFWarps * 32) k_small_warp(DevFronts F, const int32_t* list, int count,
@@ -1008,13 +1046,7 @@ __global__ void __launch_bounds__(kWFWarps * 32) k_small_warp(DevFronts F, const
   __syncwarp();
   for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
     const int c = F.child[t];
-    const int nrc = F.nr[c];
-    const T* __restrict__ U = upool + F.u_off[c];
-    const int32_t* __restrict__ loc = F.local + F.lrow_off[c];
-    for (int e = lane; e < nrc * nrc; e += 32) {           // loc is injective: no two lanes hit one entry
-      const int j = e / nrc, i = e - j * nrc;
-      if (i >= j) S[(loc[i] - 1) + (loc[j] - 1) * kWFLd] += U[i + (size_t)j * nrc];
-    }
+    extend_add_smem(S, kWFLd, upool + F.u_off[c], F.local + F.lrow_off[c], F.nr[c], lane, 32);
     __syncwarp();
   }
   T row[kWF];
@@ -1876,7 +1908,7 @@ __global__ void k_fill_int(int32_t* p, int32_t v, int64_t n) {
 inline int grid_1d(int64_t n, int threads = 256) { return clamp_grid(ceil_div(n, threads), 148 * 16); }
 
 template <typename T>
-size_t small_front_smem(int nf_max) { return (size_t)(nf_max | 1) * nf_max * sizeof(T); }
+size_t small_front_smem(int nf_max) { return ((size_t)nf_max * (nf_max + 1) / 2 + 2) * sizeof(T); }
 template <typename T>
 size_t fwd_small_smem(int nf_max) { return ((size_t)(nf_max | 1) * nf_max + 3 * nf_max) * sizeof(T); }
 

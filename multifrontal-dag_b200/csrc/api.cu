@@ -377,6 +377,7 @@ int build_plan(mfd_handle* h) {
       ll.off = push_list(h, bins[b]);
       ll.count = (int32_t)bins[b].size();
       ll.param = h->small_bins[b];
+      for (int32_t g : bins[b]) ll.param2 = std::max(ll.param2, h->fronts[g].nc);   // widest panel of the bin
       L.small.push_back(ll);
     }
     if (large.empty()) continue;
@@ -867,7 +868,7 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       double fl = 0, by = 0;
       work(s, fl, by);
       record(h, st, MFD_K_SOLVE_SMALL, fl, by,
-             [&] { launch_fwd_small<T>(F, lists + s.off, s.count, s.param, panel, X, ldx, V, nrhs, st); });
+             [&] { launch_fwd_small<T>(F, lists + s.off, s.count, s.param, s.param2, panel, X, ldx, V, nrhs, st); });
       ++n;
     }
     if (L.large.count) {
@@ -893,7 +894,7 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       double fl = 0, by = 0;
       work(s, fl, by);
       record(h, st, MFD_K_SOLVE_SMALL, fl, by,
-             [&] { launch_bwd_small<T>(F, lists + s.off, s.count, s.param, panel, X, ldx, nrhs, st); });
+             [&] { launch_bwd_small<T>(F, lists + s.off, s.count, s.param, s.param2, panel, X, ldx, nrhs, st); });
       ++n;
     }
   }

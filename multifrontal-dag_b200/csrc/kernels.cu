@@ -1910,7 +1910,9 @@ inline int grid_1d(int64_t n, int threads = 256) { return clamp_grid(ceil_div(n,
 template <typename T>
 size_t small_front_smem(int nf_max) { return ((size_t)nf_max * (nf_max + 1) / 2 + 2) * sizeof(T); }
 template <typename T>
-size_t fwd_small_smem(int nf_max) { return ((size_t)(nf_max | 1) * nf_max + 3 * nf_max) * sizeof(T); }
+size_t fwd_small_smem(int nf_max, int nc_max) {   // the panel (ld x nc) and three vectors
+  return ((size_t)(nf_max | 1) * nc_max + 3 * nf_max) * sizeof(T);
+}
 
 // Dynamic shared memory above 48 KB is opted into once per kernel at handle
 // creation (prepare_kernels), never inside a stream capture.
@@ -2038,26 +2040,26 @@ void launch_update(const DevFronts& F, const int32_t* list, int count, int step,
 }
 
 template <typename T>
-void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
-                      int64_t ldx, T* V, int nrhs, cudaStream_t st) {
+void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, int nc_max, const T* panel,
+                      T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st) {
   if (count <= 0) return;
   if (nf_max <= kWF) {
     k_fwd_small_warp<T><<<ceil_div(count, kWFWarps), kWFWarps * 32, 0, st>>>(F, list, count, panel, X, ldx, V, nrhs);
     return;
   }
-  size_t sm = fwd_small_smem<T>(nf_max);
+  size_t sm = fwd_small_smem<T>(nf_max, nc_max);
   set_smem(k_fwd_small<T>, sm);
   k_fwd_small<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, sm, st>>>(F, list, panel, X, ldx, V, nrhs);
 }
 template <typename T>
-void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
-                      int64_t ldx, int nrhs, cudaStream_t st) {
+void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, int nc_max, const T* panel,
+                      T* X, int64_t ldx, int nrhs, cudaStream_t st) {
   if (count <= 0) return;
   if (nf_max <= kWF) {
     k_bwd_small_warp<T><<<ceil_div(count, kWFWarps), kWFWarps * 32, 0, st>>>(F, list, count, panel, X, ldx, nrhs);
     return;
   }
-  size_t sm = fwd_small_smem<T>(nf_max);
+  size_t sm = fwd_small_smem<T>(nf_max, nc_max);
   set_smem(k_bwd_small<T>, sm);
   k_bwd_small<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, sm, st>>>(F, list, panel, X, ldx, nrhs);
 }
@@ -2156,9 +2158,9 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
                                bool);                                                                              \
   template void launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t,   \
                                  int, bool);                                                                       \
-  template void launch_fwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, T*, int,     \
-                                    cudaStream_t);                                                                 \
-  template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, int,         \
+  template void launch_fwd_small<T>(const DevFronts&, const int32_t*, int, int, int, const T*, T*, int64_t, T*,     \
+                                    int, cudaStream_t);                                                            \
+  template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, int, const T*, T*, int64_t, int,     \
                                     cudaStream_t);                                                                 \
   template void launch_fwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
                                     int64_t, T*, int32_t*, int, cudaStream_t, int64_t*);                           \

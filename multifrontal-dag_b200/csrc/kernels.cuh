@@ -120,11 +120,11 @@ int update_grid(int tiles, int tw, int mode);
 
 // ---- solves --------------------------------------------------------------------
 template <typename T>
-void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
-                      int64_t ldx, T* V, int nrhs, cudaStream_t st);
+void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, int nc_max, const T* panel,
+                      T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st);
 template <typename T>
-void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
-                      int64_t ldx, int nrhs, cudaStream_t st);
+void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, int nc_max, const T* panel,
+                      T* X, int64_t ldx, int nrhs, cudaStream_t st);
 // Large fronts: dinv holds the inverted 128 x 128 diagonal blocks the factorization kept (DevFronts::d_off).
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,

@@ -143,6 +143,17 @@ int mfd_factorize_solve(mfd_handle *h, const double *a, double *b, int32_t nrhs,
 
 int mfd_get_stats(mfd_handle *h, mfd_stats *st);
 
+/* Autotuner (no counterpart in the reference): times the factorization of the
+ * values `a` (host or device pointer, as for mfd_factorize) under candidate
+ * settings of the knobs that shape the schedule -- the small-front / blocked
+ * split small_front_max in {64, 96, 128, 160} and the lookahead on / off --
+ * each on a temporary handle built from h's symbolic data (one warm-up, then
+ * the median of `repeats` timed factorizations).  Writes the fastest options
+ * to *best and their factor time (ms) to *best_ms; h is left unchanged: create
+ * a handle with *best to use them.  Returns a pivot column > 0 if a
+ * factorization fails. */
+int mfd_autotune(mfd_handle *h, const double *a, int32_t repeats, mfd_options *best, double *best_ms);
+
 /* Export of the device-built index maps for parity checks.
  * which: 1 local_index (sum nr), 2 supernodal_index (nnz), 3 block-local node
  * pointer (num_node+1), 4 block pointer (groups+1), 5 parent tile numbers,

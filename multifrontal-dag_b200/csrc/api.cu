@@ -1282,6 +1282,41 @@ int mfd_solve(mfd_handle* h, double* b, int32_t nrhs, int64_t ldb, mfd_report* r
   return do_solve(h, b, nrhs, ldb, rep);
 }
 
+int mfd_autotune(mfd_handle* h, const double* a, int32_t repeats, mfd_options* best, double* best_ms) {
+  if (!h || !a || !best || repeats < 1) return fail(MFD_E_ARG, "autotune: null handle, values or output");
+  const int sfms[] = {64, 96, 128, 160};
+  double best_t = 1e300;
+  mfd_options best_o = h->opt;
+  for (int sfm : sfms) {
+    for (int lookahead_off = 0; lookahead_off <= 1; ++lookahead_off) {
+      mfd_options o = h->opt;
+      o.small_front_max = sfm;
+      o.reserved[1] = lookahead_off;
+      std::vector<Symbolic> syms = h->sys;
+      mfd_handle* t = nullptr;
+      if (create_common(&t, std::move(syms), &o) != MFD_OK) continue;   // e.g. out of memory: skip the candidate
+      std::unique_ptr<mfd_handle> guard(t);
+      int rc = do_factorize(t, a);                                      // warm-up (captures the graph)
+      if (rc != MFD_OK) return rc;
+      std::vector<double> ms;
+      for (int r = 0; r < repeats; ++r) {
+        rc = do_factorize(t, a);
+        if (rc != MFD_OK) return rc;
+        ms.push_back(t->factor_ms);
+      }
+      std::sort(ms.begin(), ms.end());
+      const double med = ms[ms.size() / 2];
+      if (med < best_t) {
+        best_t = med;
+        best_o = o;
+      }
+    }
+  }
+  *best = best_o;
+  if (best_ms) *best_ms = best_t;
+  return MFD_OK;
+}
+
 int mfd_factorize_solve(mfd_handle* h, const double* a, double* b, int32_t nrhs, int64_t ldb, mfd_report* rep) {
   int rc = mfd_factorize(h, a);
   if (rc) return rc;

@@ -65,6 +65,7 @@ class Stats(C.Structure):
 
 EXPORTS = [
     "mfd_default_options", "mfd_create", "mfd_create_batch", "mfd_analyze", "mfd_analyze_batch", "mfd_factorize",
+    "mfd_autotune",
     "mfd_solve", "mfd_factorize_solve", "mfd_get_stats", "mfd_get_index", "mfd_get_symbolic", "mfd_get_front_panel",
     "mfd_destroy", "mfd_last_error", "mfd_set_profiling", "mfd_get_profile", "mfd_factor_fronts_noalloc",
     "mfd_noalloc_last_error", "mfd_symbolic_analyze", "mfd_symbolic_view", "mfd_symbolic_free", "hppllt_init", "hppllt_set_precision", "hppllt_analyze", "hppllt_set_ordering",
@@ -103,6 +104,7 @@ def load(build_if_missing: bool = True):
     L.mfd_solve.argtypes = [vp, vp, i32, i64, C.POINTER(Report)]
     L.mfd_factorize_solve.argtypes = [vp, vp, vp, i32, i64, C.POINTER(Report)]
     L.mfd_get_stats.argtypes = [vp, C.POINTER(Stats)]
+    L.mfd_autotune.argtypes = [vp, vp, i32, C.POINTER(Options), C.POINTER(C.c_double)]
     L.mfd_get_index.restype = i64
     L.mfd_get_index.argtypes = [vp, i32, i32, vp]
     L.mfd_get_symbolic.restype = i64
@@ -289,6 +291,19 @@ class Solver:
         if rc not in (0, -5):
             _check(rc)
         return rep, rc
+
+    def autotune(self, a, repeats: int = 3):
+        """Time the factorization of `a` under the candidate schedule settings
+        (mfd_autotune) and return (options dict for Solver.analyze, factor ms)."""
+        if isinstance(a, np.ndarray):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+        best = Options()
+        ms = C.c_double()
+        rc = load().mfd_autotune(self._h, _ptr(a), int(repeats), C.byref(best), C.byref(ms))
+        if rc > 0:
+            raise MfdError(rc, "matrix is not positive definite")
+        _check(rc)
+        return {"small_front_max": best.small_front_max, "reserved": tuple(best.reserved)}, ms.value
 
     def stats(self) -> Stats:
         st = Stats()

@@ -14,13 +14,23 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
 
 
-def pytest_collection_modifyitems(config, items):
+def _has_cuda_device() -> bool:
+    """A CUDA device is visible (driver API through ctypes: no torch import)."""
+    import ctypes
     try:
-        import torch
-        has_gpu = torch.cuda.is_available()
-    except Exception:
-        has_gpu = False
-    if has_gpu:
+        cuda = ctypes.CDLL("libcuda.so.1")
+    except OSError:
+        return False
+    count = ctypes.c_int(0)
+    if cuda.cuInit(0) != 0 or cuda.cuDeviceGetCount(ctypes.byref(count)) != 0:
+        return False
+    return count.value > 0
+
+
+def pytest_collection_modifyitems(config, items):
+    if not any("gpu" in item.keywords for item in items):
+        return
+    if _has_cuda_device():
         return
     skip = pytest.mark.skip(reason="no CUDA device")
     for item in items:

@@ -206,6 +206,19 @@ def test_programmatic_launch_matches():
     assert np.array_equal(x0, x1)
 
 
+def test_autotune_picks_a_candidate():
+    """The autotuner times the schedule candidates and returns options whose
+    handle factors to the same solution quality."""
+    p = P.laplace3d(16)
+    s = gpu_for(p, max_zero=1000)
+    opts, ms = s.autotune(p.val, repeats=1)
+    assert opts["small_front_max"] in (64, 96, 128, 160) and ms > 0
+    t = gpu_for(p, max_zero=1000, **opts)
+    x = p.rhs.copy()
+    rep, rc = t.solve(x)
+    assert rc == 0 and P.backward_error(p.n, p.col, p.row, p.val, x, p.rhs) <= FP64_BWD_TOL
+
+
 def test_multiple_rhs():
     p = P.laplace2d(40)
     s = gpu_for(p)

@@ -56,6 +56,8 @@ WORKLOADS = {
                            make=lambda: P.elasticity3d(40, 4, 64), precision=1, max_zero=1000),
     "batch2000": dict(desc="2,000 shifted 2D 5-point Laplacians, sides ~ randint[16,128], shift ~ U[0,0.1], seed 3, FP64",
                       make=lambda: BatchProblem(P.laplace2d_batch(2000, 3)), precision=0, max_zero=100, batch=True),
+    "batch200": dict(desc="200 shifted 2D 5-point Laplacians (the first 200 of the 2,000-system batch), small case for profiling",
+                     make=lambda: BatchProblem(P.laplace2d_batch(2000, 3)[:200]), precision=0, max_zero=100, batch=True),
     "batch2000_fp32ir": dict(desc="2,000 shifted 2D 5-point Laplacians (seed 3), FP32 factor + FP64 refinement",
                              make=lambda: BatchProblem(P.laplace2d_batch(2000, 3)), precision=1, max_zero=100,
                              batch=True),

@@ -67,33 +67,26 @@ __device__ __forceinline__ void cp_async_t(T* dst, const T* src, bool valid) {
 }
 
 // Extend-add of one child's lower update triangle into a front held in shared
-// memory (ld ldS), by `nthreads` threads starting at index t0: each thread
-// gathers kEABatch entries (value and target, loads all in flight) before its
-// shared-memory adds.  local_index is injective, so no two entries of one
-// child share a target.
-constexpr int kEABatch = 8;
+// memory by `nthreads` threads starting at t0 (a multiple of 32 threads):
+// thread (row lane tx, column group ty) takes columns ty, ty + ny, ... and in
+// each the rows i >= j of its lane (no division, lower triangle only; the
+// unrolled row loop keeps several loads in flight).  The child's local_index
+// is first staged in shared memory (sloc, nrc entries) by the caller.
+// local_index is injective, so no two entries of one child share a target.
 // Packed lower storage (ldS < 0, nf = -ldS): column j starts at
 // j nf - j (j + 1) / 2 and holds rows j .. nf-1.
 __device__ __forceinline__ int packed_col(int j, int nf) { return j * nf - j * (j + 1) / 2; }
 
 template <typename T>
-__device__ __forceinline__ void extend_add_smem(T* S, int ldS, const T* __restrict__ U,
-                                                const int32_t* __restrict__ loc, int nrc, int t0, int nthreads) {
-  const int tot = nrc * nrc;
-  for (int e0 = t0; e0 < tot; e0 += nthreads * kEABatch) {
-    T val[kEABatch];
-    int dst[kEABatch];
-#pragma unroll
-    for (int u = 0; u < kEABatch; ++u) {
-      const int e = e0 + u * nthreads;
-      const int j = e / nrc, i = e - j * nrc;
-      const bool v = e < tot && i >= j;
-      val[u] = v ? U[i + (size_t)j * nrc] : T(0);
-      dst[u] = v ? (ldS > 0 ? (loc[i] - 1) + (loc[j] - 1) * ldS : packed_col(loc[j] - 1, -ldS) + (loc[i] - 1)) : -1;
-    }
-#pragma unroll
-    for (int u = 0; u < kEABatch; ++u)
-      if (dst[u] >= 0) S[dst[u]] += val[u];
+__device__ __forceinline__ void extend_add_smem(T* S, int ldS, const T* __restrict__ U, const int* sloc, int nrc,
+                                                int t0, int nthreads) {
+  const int tx = t0 & 31, ty = t0 >> 5, ny = nthreads >> 5;
+  for (int j = ty; j < nrc; j += ny) {
+    const int lj = sloc[j] - 1;
+    const int base = ldS > 0 ? lj * ldS : packed_col(lj, -ldS);
+    const T* Uc = U + (size_t)j * nrc;
+#pragma unroll 4
+    for (int i = j + tx; i < nrc; i += 32) S[base + sloc[i] - 1] += Uc[i];
   }
 }
 
@@ -253,9 +246,14 @@ __global__ void __launch_bounds__(256) k_small_front(DevFronts F, const int32_t*
     S[packed_col(c, nf) + r] = T(a[F.a_src[k]]);
   }
   __syncthreads();
+  int* sloc = reinterpret_cast<int*>(S + tri + 2);   // a child's local_index, staged
   for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
     const int c = F.child[t];
-    extend_add_smem(S, -nf, upool + F.u_off[c], F.local + F.lrow_off[c], F.nr[c], tid, nt);
+    const int nrc = F.nr[c];
+    const int32_t* loc = F.local + F.lrow_off[c];
+    for (int i = tid; i < nrc; i += nt) sloc[i] = loc[i];
+    __syncthreads();
+    extend_add_smem(S, -nf, upool + F.u_off[c], sloc, nrc, tid, nt);
     __syncthreads();
   }
   // unscaled right-looking elimination, two barriers per pivot: thread 0 forms
@@ -1029,6 +1027,7 @@ __global__ void __launch_bounds__(kWFWarps * 32) k_small_warp(DevFronts F, const
                                                               T* __restrict__ upool, int32_t* info) {
   __shared__ T sbuf[kWFWarps][kWF * kWFLd];
   __shared__ T cbuf[kWFWarps][2][kWF];
+  __shared__ int slocbuf[kWFWarps][kWF];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int slot = blockIdx.x * kWFWarps + warp;
   if (slot >= count) return;
@@ -1044,9 +1043,13 @@ __global__ void __launch_bounds__(kWFWarps * 32) k_small_warp(DevFronts F, const
     S[r + c * kWFLd] = T(a[F.a_src[k]]);
   }
   __syncwarp();
+  int* sloc = slocbuf[warp];
   for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
     const int c = F.child[t];
-    extend_add_smem(S, kWFLd, upool + F.u_off[c], F.local + F.lrow_off[c], F.nr[c], lane, 32);
+    const int nrc = F.nr[c];
+    if (lane < nrc) sloc[lane] = F.local[F.lrow_off[c] + lane];
+    __syncwarp();
+    extend_add_smem(S, kWFLd, upool + F.u_off[c], sloc, nrc, lane, 32);
     __syncwarp();
   }
   T row[kWF];
@@ -1908,7 +1911,9 @@ __global__ void k_fill_int(int32_t* p, int32_t v, int64_t n) {
 inline int grid_1d(int64_t n, int threads = 256) { return clamp_grid(ceil_div(n, threads), 148 * 16); }
 
 template <typename T>
-size_t small_front_smem(int nf_max) { return ((size_t)nf_max * (nf_max + 1) / 2 + 2) * sizeof(T); }
+size_t small_front_smem(int nf_max) {   // packed front, two pivot scales, a staged local_index
+  return ((size_t)nf_max * (nf_max + 1) / 2 + 2) * sizeof(T) + (size_t)nf_max * sizeof(int);
+}
 template <typename T>
 size_t fwd_small_smem(int nf_max, int nc_max) {   // the panel (ld x nc) and three vectors
   return ((size_t)(nf_max | 1) * nc_max + 3 * nf_max) * sizeof(T);

@@ -226,7 +226,7 @@ namespace {
 int small_front_max(const mfd_handle* h) {
   // fronts above 128 go to the blocked path: measured on the 64^3 Laplacian,
   // 128 is as fast as 160 (FP64) and 1.3 ms faster than 224 (FP32)
-  int lim = 128;
+  int lim = kSmallFrontMax;
   if (h->opt.small_front_max > 0) lim = std::min(lim, h->opt.small_front_max);
   return lim;
 }
@@ -379,6 +379,10 @@ int build_plan(mfd_handle* h) {
       ll.param = h->small_bins[b];
       for (int32_t g : bins[b]) ll.param2 = std::max(ll.param2, h->fronts[g].nc);   // widest panel of the bin
       L.small.push_back(ll);
+    }
+    if (!L.small.empty()) {   // the bins were pushed back to back: one list covers the level
+      L.small_all.off = L.small.front().off;
+      L.small_all.count = L.small.back().off + L.small.back().count - L.small_all.off;
     }
     if (large.empty()) continue;
     std::stable_sort(large.begin(), large.end(),
@@ -868,7 +872,7 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       double fl = 0, by = 0;
       work(s, fl, by);
       record(h, st, MFD_K_SOLVE_SMALL, fl, by,
-             [&] { launch_fwd_small<T>(F, lists + s.off, s.count, s.param, s.param2, panel, X, ldx, V, nrhs, st); });
+             [&] { launch_fwd_small<T>(F, lists + s.off, s.count, s.param, panel, X, ldx, V, nrhs, st); });
       ++n;
     }
     if (L.large.count) {
@@ -894,7 +898,7 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       double fl = 0, by = 0;
       work(s, fl, by);
       record(h, st, MFD_K_SOLVE_SMALL, fl, by,
-             [&] { launch_bwd_small<T>(F, lists + s.off, s.count, s.param, s.param2, panel, X, ldx, nrhs, st); });
+             [&] { launch_bwd_small<T>(F, lists + s.off, s.count, s.param, panel, X, ldx, nrhs, st); });
       ++n;
     }
   }

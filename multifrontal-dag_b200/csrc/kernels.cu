@@ -927,86 +927,6 @@ __global__ void __launch_bounds__(256) k_update_simt(DevFronts F, const int32_t*
 // solves
 // ============================================================================
 
-// Forward solve of a small front (one CTA): v = [x(own columns); 0] plus the
-// children's update vectors through local_index, L11 y = v1, v2 -= L21 y.
-template <typename T>
-__global__ void __launch_bounds__(256) k_fwd_small(DevFronts F, const int32_t* list, const T* __restrict__ panel,
-                                                   T* X, int64_t ldx, T* V, int nrhs) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int f = list[blockIdx.x];
-  const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr, ld = nf | 1;
-  T* L = reinterpret_cast<T*>(smem_raw);
-  T* v = L + (size_t)ld * nc;
-  T* y = v + nf;
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-  const T* P = panel + F.panel_off[f];
-  for (int j = warp; j < nc; j += nw)
-    for (int i = j + lane; i < nf; i += 32) L[i + j * ld] = P[i + (size_t)j * nf];
-  const int first = F.first[f];
-  const int rb = gridDim.y > 1 ? (int)blockIdx.y : 0, re = gridDim.y > 1 ? rb + 1 : nrhs;   // one RHS per CTA row
-  for (int r = rb; r < re; ++r) {
-    __syncthreads();
-    for (int i = tid; i < nf; i += nt) v[i] = i < nc ? X[first + i + r * ldx] : T(0);
-    __syncthreads();
-    for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
-      const int c = F.child[t];
-      const int ncc = F.nc[c], nrc = F.nr[c];
-      const T* Vc = V + F.v_off[c] * nrhs + (int64_t)r * (ncc + nrc) + ncc;
-      const int32_t* loc = F.local + F.lrow_off[c];
-      for (int i = tid; i < nrc; i += nt) v[loc[i] - 1] += Vc[i];
-      __syncthreads();
-    }
-    for (int k = 0; k < nc; ++k) {
-      const T yk = v[k] / L[k + k * ld];
-      for (int i = k + 1 + tid; i < nf; i += nt) v[i] -= L[i + k * ld] * yk;
-      if (tid == 0) y[k] = yk;
-      __syncthreads();
-    }
-    for (int i = tid; i < nc; i += nt) X[first + i + r * ldx] = y[i];
-    T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
-    for (int i = nc + tid; i < nf; i += nt) Vf[i] = v[i];
-  }
-}
-
-// Backward solve of a small front: v2 = x(L rows), t = v1 - L21^T v2,
-// L11^T y = t, x(own columns) = y.
-template <typename T>
-__global__ void __launch_bounds__(256) k_bwd_small(DevFronts F, const int32_t* list, const T* __restrict__ panel,
-                                                   T* X, int64_t ldx, int nrhs) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int f = list[blockIdx.x];
-  const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr, ld = nf | 1;
-  T* L = reinterpret_cast<T*>(smem_raw);
-  T* v = L + (size_t)ld * nc;
-  T* t = v + nf;
-  T* y = t + nc;
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-  const T* P = panel + F.panel_off[f];
-  for (int j = warp; j < nc; j += nw)
-    for (int i = j + lane; i < nf; i += 32) L[i + j * ld] = P[i + (size_t)j * nf];
-  const int first = F.first[f];
-  const int32_t* lr = F.lrow + F.lrow_off[f];
-  const int rb = gridDim.y > 1 ? (int)blockIdx.y : 0, re = gridDim.y > 1 ? rb + 1 : nrhs;   // one RHS per CTA row
-  for (int r = rb; r < re; ++r) {
-    __syncthreads();
-    for (int i = tid; i < nf; i += nt) v[i] = i < nc ? X[first + i + r * ldx] : X[lr[i - nc] + r * ldx];
-    __syncthreads();
-    for (int k = tid; k < nc; k += nt) {
-      T s = v[k];
-      for (int i = nc; i < nf; ++i) s -= L[i + k * ld] * v[i];
-      t[k] = s;
-    }
-    __syncthreads();
-    for (int k = nc - 1; k >= 0; --k) {
-      const T yk = t[k] / L[k + k * ld];
-      for (int m = tid; m < k; m += nt) t[m] -= L[k + m * ld] * yk;
-      if (tid == 0) y[k] = yk;
-      __syncthreads();
-    }
-    for (int i = tid; i < nc; i += nt) X[first + i + r * ldx] = y[i];
-  }
-}
-
 // ---- fronts with nf <= 32: one warp per front ---------------------------------
 // Four fronts per 128-thread CTA.  The front is assembled in a per-warp
 // shared buffer (A entries, then the children's update matrices through
@@ -1086,91 +1006,248 @@ __global__ void __launch_bounds__(kWFWarps * 32) k_small_warp(DevFronts F, const
   }
 }
 
-// forward solve of a warp front: v = own X + children's update vectors;
-// y = L11^{-1} v1 (lane i holds row i of the panel), v2 -= L21 y
-template <typename T>
-__global__ void __launch_bounds__(kWFWarps * 32) k_fwd_small_warp(DevFronts F, const int32_t* list, int count,
-                                                                  const T* __restrict__ panel, T* X, int64_t ldx,
-                                                                  T* V, int nrhs) {
-  __shared__ T vbuf[kWFWarps][kWF];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int slot = blockIdx.x * kWFWarps + warp;
-  if (slot >= count) return;
-  const int f = list[slot];
-  const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
-  const T* P = panel + F.panel_off[f];
-  T row[kWF];
+// ---- small-front solves: one warp per front (nf <= 32 R) ----------------------
+// Four fronts per 128-thread CTA, no CTA-wide barrier, so many fronts are in
+// flight per SM and their panel reads overlap.  The front's solve vector is
+// staged in a per-warp shared vector (the children's update vectors are
+// scattered into it through local_index).
+//   forward : lane l holds rows l + 32 q (q < R); column k of the panel is
+//             read lanes over rows (coalesced), y_k = v_k / L_kk is formed by
+//             the lane holding row k and broadcast by a shuffle, and every row
+//             below k takes v_i -= L_ik y_k.
+//   backward: 32-column blocks from the last: the rows below the block's
+//             triangle give t_k -= sum_i L_ik x_i as per-lane partial sums
+//             over rows (coalesced) reduced through a transposing per-warp
+//             tile; the 32 x 32 triangle is read lanes over rows, transposed
+//             through the same tile (lane k then holds column k) and solved
+//             by shuffles.
+constexpr int kSWarps = 4;
+constexpr int kTileLd = 33;
+
+template <typename T, int R>
+__device__ __forceinline__ T pick(const T (&a)[R], int q) {
+  T r = a[0];
 #pragma unroll
-  for (int j = 0; j < kWF; ++j) row[j] = (j < nc && lane < nf && lane >= j) ? P[lane + (size_t)j * nf] : T(0);
-  T dinv = T(1);
+  for (int p = 1; p < R; ++p)
+    if (p == q) r = a[p];
+  return r;
+}
+template <typename T, int R>
+__device__ __forceinline__ void put(T (&a)[R], int q, T v) {
 #pragma unroll
-  for (int j = 0; j < kWF; ++j)
-    if (j == lane && j < nc) dinv = T(1) / row[j];
-  T* vs = vbuf[warp];
-  for (int r = 0; r < nrhs; ++r) {
-    vs[lane] = lane < nc ? X[first + lane + r * ldx] : T(0);
-    __syncwarp();
-    for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
-      const int c = F.child[t];
-      const int ncc = F.nc[c], nrc = F.nr[c];
-      const T* Vc = V + F.v_off[c] * nrhs + (int64_t)r * (ncc + nrc) + ncc;
-      const int32_t* loc = F.local + F.lrow_off[c];
-      if (lane < nrc) vs[loc[lane] - 1] += Vc[lane];
+  for (int p = 0; p < R; ++p)
+    if (p == q) a[p] = v;
+}
+
+// v += the children's update vectors of front f (right-hand side r), child
+// metadata loaded one child per lane so the per-child chain is one load deep
+template <typename T, int R>
+__device__ __forceinline__ void gather_children(const DevFronts& F, int f, const T* V, int nrhs, int r, T* vs,
+                                                int lane) {
+  const int c0 = F.child_ptr[f], nch = F.child_ptr[f + 1] - c0;
+  for (int cb = 0; cb < nch; cb += 32) {
+    int cnc = 0, cnr = 0, clo = 0;
+    long long cvo = 0;
+    if (cb + lane < nch) {
+      const int c = F.child[c0 + cb + lane];
+      cnc = F.nc[c]; cnr = F.nr[c]; clo = F.lrow_off[c]; cvo = F.v_off[c];
+    }
+    const int m = min(32, nch - cb);
+    for (int t = 0; t < m; ++t) {
+      const int ncc = __shfl_sync(0xffffffffu, cnc, t), nrc = __shfl_sync(0xffffffffu, cnr, t);
+      const int lo = __shfl_sync(0xffffffffu, clo, t);
+      const long long vo = __shfl_sync(0xffffffffu, cvo, t);
+      const T* Vc = V + vo * nrhs + (int64_t)r * (ncc + nrc) + ncc;
+      const int32_t* loc = F.local + lo;
+      int li[R];
+      T vv[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int i = lane + 32 * q;
+        li[q] = i < nrc ? loc[i] - 1 : -1;
+        vv[q] = i < nrc ? Vc[i] : T(0);
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q)
+        if (li[q] >= 0) vs[li[q]] += vv[q];
       __syncwarp();
     }
-    T v = vs[lane];
-    __syncwarp();
-#pragma unroll
-    for (int k = 0; k < kWF; ++k) {
-      if (k >= nc) break;
-      const T yk = __shfl_sync(0xffffffffu, v * dinv, k);
-      if (lane == k) v = yk;
-      else if (lane > k) v -= row[k] * yk;
-    }
-    if (lane < nc) X[first + lane + r * ldx] = v;
-    else if (lane < nf) V[F.v_off[f] * nrhs + (int64_t)r * nf + lane] = v;
   }
 }
 
-// backward solve of a warp front: v2 = x(L rows); lane m < nc holds column m
-// of the panel: t_m = x_m - L21(:, m)^T v2, then L11^T x1 = t by shuffles
+// L2 prefetch of a front's panel (nf x nc, contiguous, 16-byte aligned; the
+// size is rounded up into the pool's alignment padding)
 template <typename T>
-__global__ void __launch_bounds__(kWFWarps * 32) k_bwd_small_warp(DevFronts F, const int32_t* list, int count,
-                                                                  const T* __restrict__ panel, T* X, int64_t ldx,
-                                                                  int nrhs) {
-  __shared__ T vbuf[kWFWarps][kWF];
+__device__ __forceinline__ void prefetch_panel(const T* P, int nf, int nc) {
+  const unsigned bytes = ((unsigned)((size_t)nf * nc * sizeof(T)) + 15u) & ~15u;
+  if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(P), "r"(bytes) : "memory");
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void fwd_small_front(const DevFronts& F, int f, const T* __restrict__ panel, T* X,
+                                                int64_t ldx, T* V, int nrhs, T* vs, int lane) {
+  const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
+  const T* P = panel + F.panel_off[f];
+  if (lane == 0) prefetch_panel(P, nf, nc);
+  T dinv[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    const int i = lane + 32 * q;
+    dinv[q] = i < nc ? T(1) / P[i + (size_t)i * nf] : T(1);
+  }
+  T* Vf = V + F.v_off[f] * nrhs;
+  const int rb = gridDim.y > 1 ? (int)blockIdx.y : 0, re = gridDim.y > 1 ? rb + 1 : nrhs;   // one RHS per CTA row
+  for (int r = rb; r < re; ++r) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int i = lane + 32 * q;
+      vs[i] = i < nc ? X[first + i + r * ldx] : T(0);
+    }
+    __syncwarp();
+    gather_children<T, R>(F, f, V, nrhs, r, vs, lane);
+    T v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = vs[lane + 32 * q];
+    __syncwarp();
+    // columns in groups of 8 with predicated (not early-exited) steps, so the
+    // group's loads issue together: one memory latency per group
+    for (int k0 = 0; k0 < nc; k0 += 32) {
+      const int qb = k0 >> 5, kn = min(32, nc - k0);
+      const T dk = pick(dinv, qb);
+      for (int g = 0; g < kn; g += 8) {
+        T l[8][R];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int k = k0 + g + u;
+          const T* Pk = P + (size_t)k * nf;
+#pragma unroll
+          for (int q = 0; q < R; ++q) {
+            const int i = lane + 32 * q;
+            l[u][q] = (g + u < kn && i > k && i < nf) ? Pk[i] : T(0);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          if (g + u < kn) {
+            const int kk = g + u, k = k0 + kk;
+            const T yk = __shfl_sync(0xffffffffu, pick(v, qb) * dk, kk);
+#pragma unroll
+            for (int q = 0; q < R; ++q)
+              if (lane + 32 * q > k) v[q] -= l[u][q] * yk;
+            if (lane == kk) put(v, qb, yk);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int i = lane + 32 * q;
+      if (i < nc) X[first + i + r * ldx] = v[q];
+      else if (i < nf) Vf[(int64_t)r * nf + i] = v[q];
+    }
+  }
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(kSWarps * 32) k_fwd_small(DevFronts F, const int32_t* list, int count,
+                                                            const T* __restrict__ panel, T* X, int64_t ldx, T* V,
+                                                            int nrhs) {
+  __shared__ T vbuf[kSWarps][32 * R];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int slot = blockIdx.x * kWFWarps + warp;
+  const int slot = blockIdx.x * kSWarps + warp;
   if (slot >= count) return;
-  const int f = list[slot];
+  fwd_small_front<T, R>(F, list[slot], panel, X, ldx, V, nrhs, vbuf[warp], lane);
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void bwd_small_front(const DevFronts& F, int f, const T* __restrict__ panel, T* X,
+                                                int64_t ldx, int nrhs, T* xs, T* tile, int lane) {
   const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
   const int32_t* lr = F.lrow + F.lrow_off[f];
   const T* P = panel + F.panel_off[f];
-  T col[kWF];                                // col[i] = L(i, lane) for i >= lane
+  if (lane == 0) prefetch_panel(P, nf, nc);
+  const int rb = gridDim.y > 1 ? (int)blockIdx.y : 0, re = gridDim.y > 1 ? rb + 1 : nrhs;   // one RHS per CTA row
+  for (int r = rb; r < re; ++r) {
 #pragma unroll
-  for (int i = 0; i < kWF; ++i) col[i] = (lane < nc && i >= lane && i < nf) ? P[i + (size_t)lane * nf] : T(0);
-  T dinv = T(1);
-#pragma unroll
-  for (int i = 0; i < kWF; ++i)
-    if (i == lane && i < nc) dinv = T(1) / col[i];
-  T* vs = vbuf[warp];
-  for (int r = 0; r < nrhs; ++r) {
-    vs[lane] = lane < nc ? X[first + lane + r * ldx] : (lane < nf ? X[lr[lane - nc] + r * ldx] : T(0));
-    __syncwarp();
-    T t = vs[lane];
-#pragma unroll
-    for (int i = 0; i < kWF; ++i)
-      if (i >= nc && i < nf) t -= col[i] * vs[i];
-    __syncwarp();
-#pragma unroll
-    for (int k = kWF - 1; k >= 0; --k) {
-      if (k >= nc) continue;
-      const T xk = __shfl_sync(0xffffffffu, t * dinv, k);
-      if (lane == k) t = xk;
-      else if (lane < k) t -= col[k] * xk;
+    for (int q = 0; q < R; ++q) {
+      const int i = lane + 32 * q;
+      xs[i] = i < nc ? X[first + i + r * ldx] : (i < nf ? X[lr[i - nc] + r * ldx] : T(0));
     }
-    if (lane < nc) X[first + lane + r * ldx] = t;
+    __syncwarp();
+    for (int b = (nc - 1) >> 5; b >= 0; --b) {
+      const int j0 = 32 * b, e = min(j0 + 32, nc), kn = e - j0;   // the block's columns [j0, e)
+      // rows below the triangle [e, nf), lanes over rows, 8 columns at a time:
+      // tile(lane, kk) = sum over the lane's rows i of L(i, j0+kk) x_i
+      for (int g = 0; g < kn; g += 8) {
+        T acc[8];
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) acc[kk] = T(0);
+        for (int i0 = e; i0 < nf; i0 += 32) {
+          const int i = i0 + lane;
+          const bool ok = i < nf;
+          const T xi = ok ? xs[i] : T(0);
+          const T* Pi = P + i + (size_t)(j0 + g) * nf;
+          T l[8];
+#pragma unroll
+          for (int kk = 0; kk < 8; ++kk) l[kk] = (ok && g + kk < kn) ? Pi[(size_t)kk * nf] : T(0);
+#pragma unroll
+          for (int kk = 0; kk < 8; ++kk) acc[kk] += l[kk] * xi;
+        }
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) tile[lane * kTileLd + g + kk] = acc[kk];
+      }
+      __syncwarp();
+      T s = T(0);                                  // columns >= kn of the tile are not written: unused
+#pragma unroll
+      for (int j = 0; j < 32; ++j) s += tile[j * kTileLd + lane];
+      __syncwarp();
+      // the triangle, read lanes over rows (row j0 + lane, columns j0 .. row)
+      // into the tile; lane k then reads column k from it
+      {
+        const int i = j0 + lane;
+        const T* Pi = P + i + (size_t)j0 * nf;
+#pragma unroll
+        for (int h = 0; h < 32; h += 16) {
+          T l[16];
+#pragma unroll
+          for (int kk = 0; kk < 16; ++kk) l[kk] = (h + kk <= lane && lane < kn) ? Pi[(size_t)(h + kk) * nf] : T(0);
+#pragma unroll
+          for (int kk = 0; kk < 16; ++kk) tile[lane * kTileLd + h + kk] = l[kk];
+        }
+      }
+      __syncwarp();
+      const T dk = lane < kn ? T(1) / tile[lane * kTileLd + lane] : T(1);
+      T t = lane < kn ? xs[j0 + lane] - s : T(0);
+#pragma unroll 8
+      for (int ii = 31; ii >= 0; --ii) {
+        if (ii >= kn) continue;
+        const T lv = tile[ii * kTileLd + lane];    // L(j0 + ii, j0 + lane)
+        const T xi = __shfl_sync(0xffffffffu, t * dk, ii);
+        if (lane == ii) t = xi;
+        else if (lane < ii) t -= lv * xi;
+      }
+      __syncwarp();
+      if (lane < kn) xs[j0 + lane] = t;
+      __syncwarp();
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int i = lane + 32 * q;
+      if (i < nc) X[first + i + r * ldx] = xs[i];
+    }
+    __syncwarp();
   }
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(kSWarps * 32, 6) k_bwd_small(DevFronts F, const int32_t* list, int count,
+                                                            const T* __restrict__ panel, T* X, int64_t ldx, int nrhs) {
+  __shared__ T xbuf[kSWarps][32 * R];
+  __shared__ T tbuf[kSWarps][32 * kTileLd];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int slot = blockIdx.x * kSWarps + warp;
+  if (slot >= count) return;
+  bwd_small_front<T, R>(F, list[slot], panel, X, ldx, nrhs, xbuf[warp], tbuf[warp], lane);
 }
 
 // ---- large fronts: the solve vector of front f lives in V (nf per RHS) --------
@@ -1914,10 +1991,6 @@ template <typename T>
 size_t small_front_smem(int nf_max) {   // packed front, two pivot scales, a staged local_index
   return ((size_t)nf_max * (nf_max + 1) / 2 + 2) * sizeof(T) + (size_t)nf_max * sizeof(int);
 }
-template <typename T>
-size_t fwd_small_smem(int nf_max, int nc_max) {   // the panel (ld x nc) and three vectors
-  return ((size_t)(nf_max | 1) * nc_max + 3 * nf_max) * sizeof(T);
-}
 
 // Dynamic shared memory above 48 KB is opted into once per kernel at handle
 // creation (prepare_kernels), never inside a stream capture.
@@ -1943,8 +2016,6 @@ cudaError_t prepare_kernels() {
   chk(opt_in(k_potrf<double>)); chk(opt_in(k_potrf<float>));
   chk(prepare_update_tc());
   chk(opt_in(k_update_simt<double>)); chk(opt_in(k_update_simt<float>));
-  chk(opt_in(k_fwd_small<double>)); chk(opt_in(k_fwd_small<float>));
-  chk(opt_in(k_bwd_small<double>)); chk(opt_in(k_bwd_small<float>));
   return e;
 }
 
@@ -2044,29 +2115,30 @@ void launch_update(const DevFronts& F, const int32_t* list, int count, int step,
   k_update_simt<T><<<dim3(g, count), 256, sm, st>>>(F, list, step, panel, upool, mode);
 }
 
+// one launch per size bin (nf_max <= 32 R, R <= kSmallFrontMax / 32 = 4)
 template <typename T>
-void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, int nc_max, const T* panel,
-                      T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st) {
+void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
+                      int64_t ldx, T* V, int nrhs, cudaStream_t st) {
   if (count <= 0) return;
-  if (nf_max <= kWF) {
-    k_fwd_small_warp<T><<<ceil_div(count, kWFWarps), kWFWarps * 32, 0, st>>>(F, list, count, panel, X, ldx, V, nrhs);
-    return;
+  const dim3 grid(ceil_div(count, kSWarps), nrhs >= kMrhsMin ? nrhs : 1), block(kSWarps * 32);
+  switch (ceil_div(nf_max, 32)) {
+    case 1: k_fwd_small<T, 1><<<grid, block, 0, st>>>(F, list, count, panel, X, ldx, V, nrhs); break;
+    case 2: k_fwd_small<T, 2><<<grid, block, 0, st>>>(F, list, count, panel, X, ldx, V, nrhs); break;
+    case 3: k_fwd_small<T, 3><<<grid, block, 0, st>>>(F, list, count, panel, X, ldx, V, nrhs); break;
+    default: k_fwd_small<T, 4><<<grid, block, 0, st>>>(F, list, count, panel, X, ldx, V, nrhs); break;
   }
-  size_t sm = fwd_small_smem<T>(nf_max, nc_max);
-  set_smem(k_fwd_small<T>, sm);
-  k_fwd_small<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, sm, st>>>(F, list, panel, X, ldx, V, nrhs);
 }
 template <typename T>
-void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, int nc_max, const T* panel,
-                      T* X, int64_t ldx, int nrhs, cudaStream_t st) {
+void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
+                      int64_t ldx, int nrhs, cudaStream_t st) {
   if (count <= 0) return;
-  if (nf_max <= kWF) {
-    k_bwd_small_warp<T><<<ceil_div(count, kWFWarps), kWFWarps * 32, 0, st>>>(F, list, count, panel, X, ldx, nrhs);
-    return;
+  const dim3 grid(ceil_div(count, kSWarps), nrhs >= kMrhsMin ? nrhs : 1), block(kSWarps * 32);
+  switch (ceil_div(nf_max, 32)) {
+    case 1: k_bwd_small<T, 1><<<grid, block, 0, st>>>(F, list, count, panel, X, ldx, nrhs); break;
+    case 2: k_bwd_small<T, 2><<<grid, block, 0, st>>>(F, list, count, panel, X, ldx, nrhs); break;
+    case 3: k_bwd_small<T, 3><<<grid, block, 0, st>>>(F, list, count, panel, X, ldx, nrhs); break;
+    default: k_bwd_small<T, 4><<<grid, block, 0, st>>>(F, list, count, panel, X, ldx, nrhs); break;
   }
-  size_t sm = fwd_small_smem<T>(nf_max, nc_max);
-  set_smem(k_bwd_small<T>, sm);
-  k_bwd_small<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, sm, st>>>(F, list, panel, X, ldx, nrhs);
 }
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
@@ -2163,9 +2235,9 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
                                bool);                                                                              \
   template void launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t,   \
                                  int, bool);                                                                       \
-  template void launch_fwd_small<T>(const DevFronts&, const int32_t*, int, int, int, const T*, T*, int64_t, T*,     \
-                                    int, cudaStream_t);                                                            \
-  template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, int, const T*, T*, int64_t, int,     \
+  template void launch_fwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, T*, int,    \
+                                    cudaStream_t);                                                                 \
+  template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, int,         \
                                     cudaStream_t);                                                                 \
   template void launch_fwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
                                     int64_t, T*, int32_t*, int, cudaStream_t, int64_t*);                           \

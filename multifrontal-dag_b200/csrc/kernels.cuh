@@ -11,6 +11,7 @@
 
 namespace mfd {
 
+constexpr int kSmallFrontMax = 128;   // widest front of the one-CTA / one-warp small-front kernels
 constexpr int kFactB = 128;          // column panel of the blocked large-front factorization
 constexpr int kTrRowsH = 64;         // rows per CTA of the panel TRSM
 constexpr int kUpdTile = 128;        // trailing-update output tile (tensor path)
@@ -119,12 +120,13 @@ void launch_update_tc(const DevFronts& F, const int32_t* list, int count, int st
 int update_grid(int tiles, int tw, int mode);
 
 // ---- solves --------------------------------------------------------------------
+// Small fronts (one size bin, nf <= nf_max <= kSmallFrontMax): one warp per front.
 template <typename T>
-void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, int nc_max, const T* panel,
-                      T* X, int64_t ldx, T* V, int nrhs, cudaStream_t st);
+void launch_fwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
+                      int64_t ldx, T* V, int nrhs, cudaStream_t st);
 template <typename T>
-void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, int nc_max, const T* panel,
-                      T* X, int64_t ldx, int nrhs, cudaStream_t st);
+void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
+                      int64_t ldx, int nrhs, cudaStream_t st);
 // Large fronts: dinv holds the inverted 128 x 128 diagonal blocks the factorization kept (DevFronts::d_off).
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,

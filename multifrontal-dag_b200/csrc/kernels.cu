@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -224,11 +225,19 @@ __global__ void k_bli_fill(DevFronts F, const int32_t* fronts, int count, int nb
 // factorization
 // ============================================================================
 
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int kSfW = 8;   // panel width of the small-front elimination
+
 // Fused small front: zero, assemble A, extend-add the children in order, partial
 // Cholesky of the nc supernode columns and the Schur complement, all in shared
 // memory; writes the factor panel and the update matrix once.
 template <typename T>
-__global__ void __launch_bounds__(256) k_small_front(DevFronts F, const int32_t* list, const double* __restrict__ a,
+__global__ void __launch_bounds__(256, 8) k_small_front(DevFronts F, const int32_t* list, const double* __restrict__ a,
                                                      T* __restrict__ panel, T* __restrict__ upool, int32_t* info) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S = reinterpret_cast<T*>(smem_raw);     // the front's lower triangle, packed by columns
@@ -256,35 +265,113 @@ __global__ void __launch_bounds__(256) k_small_front(DevFronts F, const int32_t*
     extend_add_smem(S, -nf, upool + F.u_off[c], sloc, nrc, tid, nt);
     __syncthreads();
   }
-  // unscaled right-looking elimination, two barriers per pivot: thread 0 forms
-  // y_k = 1/sqrt(d_k); then the trailing part takes -c_i c_j y_k^2 from the
-  // still unscaled column k while column k-1 is scaled to L(:, k-1)
-  T* ys = S + tri;                           // two pivot scales after the front
-  for (int k = 0; k < nc; ++k) {
-    T* colk = S + packed_col(k, nf);
-    if (tid == 0) {
-      T d = colk[k];
-      if (!(d > T(0))) { atomicMin(info, F.first[f] + k + 1); d = T(1); colk[k] = d; }
-      ys[k & 1] = rsqrt_t<T>(d);
+  // blocked right-looking elimination, panels of kSfW columns, three barriers
+  // per panel: (1) lanes 0..w-1 of warp 0 factor the w x w diagonal block in
+  // registers (lane = row, pivots by shuffles); (2) every thread solves rows
+  // of the block column below it, l_ip = (a_ip - sum_{p'<p} l_ip' L_pp') y_p;
+  // (3) the rank-w update S_ij -= sum_p L_ip L_jp of the trailing triangle
+  // (FP64: 8 x 8 tiles on m8n8k4 DMMA, one warp per tile; FP32: warps over
+  // columns, lanes over rows)
+  T* ys = S + tri;                           // the panel's pivot scales y_p = 1/sqrt(d_p)
+  for (int k0 = 0; k0 < nc; k0 += kSfW) {
+    const int w = min(kSfW, nc - k0);
+    int pc[kSfW];
+#pragma unroll
+    for (int p = 0; p < kSfW; ++p) pc[p] = packed_col(k0 + min(p, w - 1), nf);
+    if (warp == 0) {
+      T rv[kSfW];
+      const int r = k0 + lane;
+#pragma unroll
+      for (int p = 0; p < kSfW; ++p) rv[p] = (lane < w && p < w && p <= lane) ? S[pc[p] + r] : T(0);
+#pragma unroll
+      for (int p = 0; p < kSfW; ++p) {
+        if (p < w) {
+          T d = __shfl_sync(0xffffffffu, rv[p], p);
+          if (!(d > T(0))) {
+            if (lane == 0) atomicMin(info, F.first[f] + k0 + p + 1);
+            d = T(1);
+          }
+          const T y = rsqrt_t<T>(d);
+          if (lane > p) rv[p] *= y;
+          else if (lane == p) { rv[p] = d * y; ys[p] = y; }
+#pragma unroll
+          for (int p2 = p + 1; p2 < kSfW; ++p2) {
+            if (p2 < w) {
+              const T lj = __shfl_sync(0xffffffffu, rv[p], p2);
+              if (lane >= p2) rv[p2] -= rv[p] * lj;
+            }
+          }
+        }
+      }
+      if (lane < w) {
+#pragma unroll
+        for (int p = 0; p < kSfW; ++p)
+          if (p <= lane) S[pc[p] + r] = rv[p];
+      }
     }
     __syncthreads();
-    const T y = ys[k & 1], y2 = y * y;
-    for (int j = k + 1 + warp; j < nf; j += nw) {
-      const T cj = colk[j] * y2;
-      T* colj = S + packed_col(j, nf);
-      for (int i = j + lane; i < nf; i += 32) colj[i] -= colk[i] * cj;
-    }
-    if (k > 0) {
-      T* colp = S + packed_col(k - 1, nf);
-      const T yp = ys[(k - 1) & 1];
-      for (int i = k - 1 + tid; i < nf; i += nt) colp[i] *= yp;      // diagonal: d y = sqrt(d)
+    for (int i = k0 + w + tid; i < nf; i += nt) {
+      T x[kSfW];
+#pragma unroll
+      for (int p = 0; p < kSfW; ++p) x[p] = p < w ? S[pc[p] + i] : T(0);
+#pragma unroll
+      for (int p = 0; p < kSfW; ++p) {
+        if (p < w) {
+          T v = x[p];
+#pragma unroll
+          for (int q = 0; q < p; ++q) v -= x[q] * S[pc[q] + k0 + p];
+          x[p] = v * ys[p];
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < kSfW; ++p)
+        if (p < w) S[pc[p] + i] = x[p];
     }
     __syncthreads();
-  }
-  if (nc > 0) {
-    T* colp = S + packed_col(nc - 1, nf);
-    const T yp = ys[(nc - 1) & 1];
-    for (int i = nc - 1 + tid; i < nf; i += nt) colp[i] *= yp;
+    const int kb = k0 + w;                   // the trailing triangle: rows and columns [kb, nf)
+    if constexpr (std::is_same<T, double>::value) {
+      const int t8 = (nf - kb + 7) >> 3, tiles = t8 * (t8 + 1) / 2;
+      const int g = lane >> 2, q = lane & 3;
+      for (int t = warp; t < tiles; t += nw) {
+        int ti = 0;                          // tile (ti, tj), ti >= tj, row-major over the lower triangle
+        while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+        const int tj = t - ti * (ti + 1) / 2;
+        const int i0 = kb + 8 * ti, j0 = kb + 8 * tj;
+        const int ia = i0 + g, jb = j0 + g;  // the row of A and the column of B this lane feeds
+        double c[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int j = j0 + 2 * q + e;
+          c[e] = (ia < nf && j < nf && ia >= j) ? S[packed_col(j, nf) + ia] : 0.0;
+        }
+#pragma unroll
+        for (int s4 = 0; s4 < kSfW; s4 += 4) {
+          const int p = s4 + q;
+          const double av = (p < w && ia < nf) ? -S[pc[p] + ia] : 0.0;
+          const double bv = (p < w && jb < nf) ? S[pc[p] + jb] : 0.0;
+          dmma(c[0], c[1], av, bv);
+        }
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int j = j0 + 2 * q + e;
+          if (ia < nf && j < nf && ia >= j) S[packed_col(j, nf) + ia] = c[e];
+        }
+      }
+    } else {
+      for (int j = kb + warp; j < nf; j += nw) {
+        T lj[kSfW];
+#pragma unroll
+        for (int p = 0; p < kSfW; ++p) lj[p] = p < w ? S[pc[p] + j] : T(0);
+        T* colj = S + packed_col(j, nf);
+        for (int i = j + lane; i < nf; i += 32) {
+          T acc = colj[i];
+#pragma unroll
+          for (int p = 0; p < kSfW; ++p)
+            if (p < w) acc -= S[pc[p] + i] * lj[p];
+          colj[i] = acc;
+        }
+      }
+    }
     __syncthreads();
   }
   T* P = panel + F.panel_off[f];
@@ -389,11 +476,6 @@ constexpr size_t kPotrfSmem =
     sizeof(double) * ((size_t)kFactB * kPLd + (size_t)(kFactB / kPSub) * kPSub * kDLd +
                       (size_t)(kFactB / kPSub - 1) * kPSub * kDLd + kFactB + 2 * kPSub);
 
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
 
 // One warp: acc(8 MF x 32) += A(8 MF x K) B(K x 32), K a multiple of 4, operands
 // in shared memory addressed as A(i, k) = A[i * ai + k * ak] and

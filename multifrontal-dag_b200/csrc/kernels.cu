@@ -78,8 +78,44 @@ __device__ __forceinline__ void cp_async_t(T* dst, const T* src, bool valid) {
 // j nf - j (j + 1) / 2 and holds rows j .. nf-1.
 __device__ __forceinline__ int packed_col(int j, int nf) { return j * nf - j * (j + 1) / 2; }
 
+// S(local) += U for one child's update matrix U (nrc x nrc, lower triangle,
+// column-major) through its staged local_index sloc: lanes over rows, warps
+// over columns, CU columns x RI row passes of loads issued together per
+// chunk (predicated, no early exit), then the shared-memory adds.  ldS > 0:
+// S column-major with leading dimension ldS; ldS < 0: S packed (nf = -ldS).
+template <typename T, int RI, int CU>
+__device__ __forceinline__ void extend_add_chunk(T* S, int ldS, const T* __restrict__ U, const int* sloc, int nrc,
+                                                 int tx, int ty, int ny) {
+  for (int j0 = ty; j0 < nrc; j0 += CU * ny) {
+    T u[CU][RI];
+#pragma unroll
+    for (int c = 0; c < CU; ++c) {
+      const int j = j0 + c * ny;
+#pragma unroll
+      for (int v = 0; v < RI; ++v) {
+        const int i = j + tx + 32 * v;
+        u[c][v] = (j < nrc && i < nrc) ? U[(size_t)j * nrc + i] : T(0);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CU; ++c) {
+      const int j = j0 + c * ny;
+      if (j < nrc) {
+        const int lj = sloc[j] - 1;
+        const int base = ldS > 0 ? lj * ldS : packed_col(lj, -ldS);
+#pragma unroll
+        for (int v = 0; v < RI; ++v) {
+          const int i = j + tx + 32 * v;
+          if (i < nrc) S[base + sloc[i] - 1] += u[c][v];
+        }
+      }
+    }
+  }
+}
+// The same scatter with one column per warp step (lanes over rows): the
+// one-CTA-per-front kernel, whose 8 warps already keep 8 columns in flight.
 template <typename T>
-__device__ __forceinline__ void extend_add_smem(T* S, int ldS, const T* __restrict__ U, const int* sloc, int nrc,
+__device__ __forceinline__ void extend_add_cols(T* S, int ldS, const T* __restrict__ U, const int* sloc, int nrc,
                                                 int t0, int nthreads) {
   const int tx = t0 & 31, ty = t0 >> 5, ny = nthreads >> 5;
   for (int j = ty; j < nrc; j += ny) {
@@ -88,6 +124,46 @@ __device__ __forceinline__ void extend_add_smem(T* S, int ldS, const T* __restri
     const T* Uc = U + (size_t)j * nrc;
 #pragma unroll 4
     for (int i = j + tx; i < nrc; i += 32) S[base + sloc[i] - 1] += Uc[i];
+  }
+}
+// NB: loads in flight per thread and chunk (register budget)
+template <int NB, typename T>
+__device__ __forceinline__ void extend_add_smem(T* S, int ldS, const T* __restrict__ U, const int* sloc, int nrc,
+                                                int t0, int nthreads) {
+  const int tx = t0 & 31, ty = t0 >> 5, ny = nthreads >> 5;
+  switch ((nrc + 31) >> 5) {                 // row passes a column needs (nrc <= 128)
+    case 0: break;
+    case 1: extend_add_chunk<T, 1, NB>(S, ldS, U, sloc, nrc, tx, ty, ny); break;
+    case 2: extend_add_chunk<T, 2, (NB / 2 > 0 ? NB / 2 : 1)>(S, ldS, U, sloc, nrc, tx, ty, ny); break;
+    case 3: extend_add_chunk<T, 3, (NB / 3 > 0 ? NB / 3 : 1)>(S, ldS, U, sloc, nrc, tx, ty, ny); break;
+    default: extend_add_chunk<T, 4, (NB / 4 > 0 ? NB / 4 : 1)>(S, ldS, U, sloc, nrc, tx, ty, ny); break;
+  }
+}
+
+// A's entries of front f into its shared buffer (entry position pos = row +
+// col * nf, row >= col, placed at S[addr(row, col)]), U entries per thread
+// with their loads in flight together
+template <int UN, typename T, typename Addr>
+__device__ __forceinline__ void assemble_smem(const DevFronts& F, int f, int nf, const double* __restrict__ a, T* S,
+                                              Addr addr, int t0, int nthreads) {
+  const int a0 = F.a_beg[f], a1 = F.a_beg[f + 1];
+  for (int k0 = a0 + t0; k0 < a1; k0 += UN * nthreads) {
+    int pos[UN], src[UN];
+#pragma unroll
+    for (int u = 0; u < UN; ++u) {
+      const int k = k0 + u * nthreads;
+      pos[u] = k < a1 ? F.a_pos[k] : -1;
+      src[u] = k < a1 ? F.a_src[k] : 0;
+    }
+    double v[UN];
+#pragma unroll
+    for (int u = 0; u < UN; ++u) v[u] = pos[u] >= 0 ? a[src[u]] : 0.0;
+#pragma unroll
+    for (int u = 0; u < UN; ++u)
+      if (pos[u] >= 0) {
+        const int c = pos[u] / nf, r = pos[u] - c * nf;
+        S[addr(r, c)] = T(v[u]);
+      }
   }
 }
 
@@ -262,7 +338,7 @@ __global__ void __launch_bounds__(256, 8) k_small_front(DevFronts F, const int32
     const int32_t* loc = F.local + F.lrow_off[c];
     for (int i = tid; i < nrc; i += nt) sloc[i] = loc[i];
     __syncthreads();
-    extend_add_smem(S, -nf, upool + F.u_off[c], sloc, nrc, tid, nt);
+    extend_add_cols(S, -nf, upool + F.u_off[c], sloc, nrc, tid, nt);
     __syncthreads();
   }
   // blocked right-looking elimination, panels of kSfW columns, three barriers
@@ -1038,12 +1114,7 @@ __global__ void __launch_bounds__(kWFWarps * 32) k_small_warp(DevFronts F, const
   T* S = sbuf[warp];
   for (int e = lane; e < kWF * kWFLd; e += 32) S[e] = T(0);
   __syncwarp();
-  const int a0 = F.a_beg[f], a1 = F.a_beg[f + 1];
-  for (int k = a0 + lane; k < a1; k += 32) {
-    const int pos = F.a_pos[k];
-    const int c = pos / nf, r = pos - c * nf;
-    S[r + c * kWFLd] = T(a[F.a_src[k]]);
-  }
+  assemble_smem<4>(F, f, nf, a, S, [](int r, int c) { return r + c * kWFLd; }, lane, 32);
   __syncwarp();
   int* sloc = slocbuf[warp];
   for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
@@ -1051,7 +1122,7 @@ __global__ void __launch_bounds__(kWFWarps * 32) k_small_warp(DevFronts F, const
     const int nrc = F.nr[c];
     if (lane < nrc) sloc[lane] = F.local[F.lrow_off[c] + lane];
     __syncwarp();
-    extend_add_smem(S, kWFLd, upool + F.u_off[c], sloc, nrc, lane, 32);
+    extend_add_smem<8>(S, kWFLd, upool + F.u_off[c], sloc, nrc, lane, 32);
     __syncwarp();
   }
   T row[kWF];

@@ -857,6 +857,9 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
   const double w = sizeof(T);
   const bool prof = h->profiling;
   const int32_t* hl = h->h_lists.data();
+  // programmatic dependent launch between the large-front solve steps (on
+  // unless reserved[3] = 1; the profiling schedule times kernels one by one)
+  const bool solve_pdl = h->opt.reserved[3] != 1 && !prof;
   // algorithmic work of one sweep over a list: read the panel once, 2 flops per entry per RHS
   auto work = [&](const LaunchList& l, double& fl, double& by) {
     if (!prof) return;
@@ -880,7 +883,7 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       work(L.large, fl, by);
       record(h, st, MFD_K_SOLVE_LARGE, fl, by, [&] {
         launch_fwd_large<T>(F, lists + L.large.off, L.large.count, L.large.param2, L.large_max_nf, panel, dinv, X,
-                            ldx, V, h->d_cnt.p, nrhs, st, &n);
+                            ldx, V, h->d_cnt.p, nrhs, st, &n, solve_pdl);
       });
     }
   }
@@ -891,7 +894,7 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       work(L.large, fl, by);
       record(h, st, MFD_K_SOLVE_LARGE, fl, by, [&] {
         launch_bwd_large<T>(F, lists + L.large.off, L.large.count, L.large.param2, L.large_max_nf, panel, dinv, X,
-                            ldx, V, S, h->d_cnt.p, nrhs, st, &n);
+                            ldx, V, S, h->d_cnt.p, nrhs, st, &n, solve_pdl);
       });
     }
     for (const LaunchList& s : L.small) {

@@ -323,6 +323,9 @@ __global__ void __launch_bounds__(256, 8) k_small_front(DevFronts F, const int32
   const int tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
 
+  // shared memory: the packed front (tri), kSfW pivot scales, a child's
+  // local_index (nf ints)
+  int* sloc = reinterpret_cast<int*>(S + tri + kSfW);
   for (int i = tid; i < tri; i += nt) S[i] = T(0);
   __syncthreads();
   for (int k = F.a_beg[f] + tid; k < F.a_beg[f + 1]; k += nt) {
@@ -331,7 +334,6 @@ __global__ void __launch_bounds__(256, 8) k_small_front(DevFronts F, const int32
     S[packed_col(c, nf) + r] = T(a[F.a_src[k]]);
   }
   __syncthreads();
-  int* sloc = reinterpret_cast<int*>(S + tri + 2);   // a child's local_index, staged
   for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
     const int c = F.child[t];
     const int nrc = F.nr[c];
@@ -1112,18 +1114,37 @@ __global__ void __launch_bounds__(kWFWarps * 32) k_small_warp(DevFronts F, const
   const int f = list[slot];
   const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
   T* S = sbuf[warp];
+  // children's metadata one per lane (broadcast by shuffles), loaded while
+  // the front is zeroed and assembled
+  const int cp0 = F.child_ptr[f], nch = F.child_ptr[f + 1] - cp0;
+  int cnr = 0, clo = 0;
+  long long cuo = 0;
+  if (lane < nch) {
+    const int c = F.child[cp0 + lane];
+    cnr = F.nr[c]; clo = F.lrow_off[c]; cuo = F.u_off[c];
+  }
   for (int e = lane; e < kWF * kWFLd; e += 32) S[e] = T(0);
   __syncwarp();
   assemble_smem<4>(F, f, nf, a, S, [](int r, int c) { return r + c * kWFLd; }, lane, 32);
   __syncwarp();
   int* sloc = slocbuf[warp];
-  for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
-    const int c = F.child[t];
-    const int nrc = F.nr[c];
-    if (lane < nrc) sloc[lane] = F.local[F.lrow_off[c] + lane];
-    __syncwarp();
-    extend_add_smem<8>(S, kWFLd, upool + F.u_off[c], sloc, nrc, lane, 32);
-    __syncwarp();
+  for (int cb = 0; cb < nch; cb += 32) {
+    if (cb > 0) {
+      cnr = 0; clo = 0; cuo = 0;
+      if (cb + lane < nch) {
+        const int c = F.child[cp0 + cb + lane];
+        cnr = F.nr[c]; clo = F.lrow_off[c]; cuo = F.u_off[c];
+      }
+    }
+    const int m = min(32, nch - cb);
+    for (int t = 0; t < m; ++t) {
+      const int nrc = __shfl_sync(0xffffffffu, cnr, t), lo = __shfl_sync(0xffffffffu, clo, t);
+      const long long uo = __shfl_sync(0xffffffffu, cuo, t);
+      if (lane < nrc) sloc[lane] = F.local[lo + lane];
+      __syncwarp();
+      extend_add_smem<8>(S, kWFLd, upool + uo, sloc, nrc, lane, 32);
+      __syncwarp();
+    }
   }
   T row[kWF];
 #pragma unroll
@@ -1510,6 +1531,8 @@ __global__ void __launch_bounds__(256) k_fwd_large_rest(DevFronts F, const int32
   __shared__ int last;
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nf = nc + F.nr[f];
+  pdl_wait();            // the previous step (or gather) of the sweep has completed
+  pdl_trigger();
   const int c0 = step * kSolveB;
   if (c0 >= nc) return;
   const int w = min(kSolveB, nc - c0);
@@ -1715,6 +1738,8 @@ __global__ void __launch_bounds__(256) k_bwd_large_step(DevFronts F, const int32
   __shared__ int last;
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nf = nc + F.nr[f];
+  pdl_wait();            // the previous step (or gather) of the sweep has completed
+  pdl_trigger();
   const int c0 = step * kSolveB;
   if (c0 >= nc) return;
   const int w = min(kSolveB, nc - c0);
@@ -2141,8 +2166,8 @@ __global__ void k_fill_int(int32_t* p, int32_t v, int64_t n) {
 inline int grid_1d(int64_t n, int threads = 256) { return clamp_grid(ceil_div(n, threads), 148 * 16); }
 
 template <typename T>
-size_t small_front_smem(int nf_max) {   // packed front, two pivot scales, a staged local_index
-  return ((size_t)nf_max * (nf_max + 1) / 2 + 2) * sizeof(T) + (size_t)nf_max * sizeof(int);
+size_t small_front_smem(int nf_max) {   // packed front, kSfW pivot scales, a staged local_index
+  return ((size_t)nf_max * (nf_max + 1) / 2 + kSfW) * sizeof(T) + (size_t)nf_max * sizeof(int);
 }
 
 // Dynamic shared memory above 48 KB is opted into once per kernel at handle
@@ -2296,7 +2321,7 @@ void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
                       const T* dinv, T* X, int64_t ldx, T* V, int32_t* cnt, int nrhs, cudaStream_t st,
-                      int64_t* launches) {
+                      int64_t* launches, bool pdl) {
   if (count <= 0) return;
   k_fwd_large_gather<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, 0, st>>>(F, list, dinv, X, ldx, V, nrhs);
   const int steps = ceil_div(max_nc, kSolveB);
@@ -2311,13 +2336,14 @@ void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int ma
   }
   const int chunks = std::max(1, ceil_div(max_nf, kFwdRows));
   for (int s = 0; s < steps; ++s)
-    k_fwd_large_rest<T><<<dim3(chunks, count), 256, 0, st>>>(F, list, s, panel, dinv, X, ldx, V, cnt, nrhs);
+    launch_k(k_fwd_large_rest<T>, dim3(chunks, count), dim3(256), 0, st, pdl, F, list, s, panel, dinv, X, ldx, V, cnt,
+             nrhs);
   if (launches) *launches += 1 + steps;
 }
 template <typename T>
 void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
                       const T* dinv, T* X, int64_t ldx, T* V, T* scratch, int32_t* cnt, int nrhs, cudaStream_t st,
-                      int64_t* launches) {
+                      int64_t* launches, bool pdl) {
   if (count <= 0) return;
   k_bwd_large_gather<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, 0, st>>>(F, list, X, ldx, V, nrhs);
   const int steps = ceil_div(max_nc, kSolveB);
@@ -2335,7 +2361,8 @@ void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int ma
     return;
   }
   for (int s = steps - 1; s >= 0; --s)
-    k_bwd_large_step<T><<<dim3(chunks, count), 256, 0, st>>>(F, list, s, panel, dinv, X, ldx, V, scratch, cnt, nrhs);
+    launch_k(k_bwd_large_step<T>, dim3(chunks, count), dim3(256), 0, st, pdl, F, list, s, panel, dinv, X, ldx, V,
+             scratch, cnt, nrhs);
   if (launches) *launches += 1 + steps;
 }
 
@@ -2393,9 +2420,9 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
   template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, int,         \
                                     cudaStream_t);                                                                 \
   template void launch_fwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
-                                    int64_t, T*, int32_t*, int, cudaStream_t, int64_t*);                           \
+                                    int64_t, T*, int32_t*, int, cudaStream_t, int64_t*, bool);                     \
   template void launch_bwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
-                                    int64_t, T*, T*, int32_t*, int, cudaStream_t, int64_t*);                       \
+                                    int64_t, T*, T*, int32_t*, int, cudaStream_t, int64_t*, bool);                 \
   template void launch_permute_in<T>(const double*, int64_t, const int32_t*, T*, int64_t, int64_t, int,            \
                                      cudaStream_t);                                                                \
   template void launch_permute_out<T>(const T*, int64_t, const int32_t*, double*, int64_t, int64_t, int,           \

@@ -131,12 +131,14 @@ void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
                       const T* dinv, T* X, int64_t ldx, T* V, int32_t* cnt, int nrhs, cudaStream_t st,
-                      int64_t* launches);
+                      int64_t* launches, bool pdl);
 // cnt: one zero-initialised ticket per list slot (left zero again on exit)
 template <typename T>
 void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
                       const T* dinv, T* X, int64_t ldx, T* V, T* scratch, int32_t* cnt, int nrhs, cudaStream_t st,
-                      int64_t* launches);
+                      int64_t* launches, bool pdl);
+// pdl: the single-RHS step kernels go out with programmatic dependent launch
+// (each waits for its predecessor before reading the sweep's vectors)
 
 // ---- vectors, residuals ---------------------------------------------------------
 template <typename T>

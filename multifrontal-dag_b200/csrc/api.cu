@@ -319,7 +319,7 @@ int build_plan(mfd_handle* h) {
     if (nf > sfm) h->dinv_elems += (int64_t)((fr.nc + kFactB - 1) / kFactB) * kFactB * kFactB;   // kept for the solves
   }
   // large-front solve partials: one region per level (levels solve one after
-  // another), kMrhsRows-row chunks cover the single-RHS 256-row chunks too
+  // another), kMrhsRows-row chunks (the single-RHS backward uses the same 64)
   {
     std::vector<int64_t> used(nlev, 0);
     for (int32_t g = 0; g < nfr; ++g) {

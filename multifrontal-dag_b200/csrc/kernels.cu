@@ -1430,7 +1430,7 @@ __global__ void __launch_bounds__(kSWarps * 32, 6) k_bwd_small(DevFronts F, cons
 //   forward : v_rest -= L_rest,s y_s over 32-row chunks (k_fwd_large_rest);
 //             the last CTA of the front to finish (ticket) then forms the next
 //             step's y_{s+1} = Li v_{s+1}; y_0 is formed by the gather kernel
-//   backward: t_s = v_s - L_rest,s^T x_rest, partial sums per 256-row chunk;
+//   backward: t_s = v_s - L_rest,s^T x_rest, partial sums per 64-row chunk;
 //             the last CTA sums them in chunk order (deterministic) and forms
 //             x_s = Li^T t_s (k_bwd_large_step)
 // The diagonal solves write the front's own entries of X directly.
@@ -1599,131 +1599,14 @@ __global__ void k_bwd_large_gather(DevFronts F, const int32_t* list, const T* X,
   }
 }
 
-// partial sums of L_rest,s^T x_rest over one 256-row chunk: warp q takes rows
-// 32q .. 32q+31 of the chunk (lane = row, coalesced column reads),
-// 16 columns at a time for up to 4 right-hand sides, then a butterfly
-// transpose-reduce leaves column kb + (l mod 16)'s sum in lane l
-constexpr int kBwdG = 4;
-template <typename T>
-__global__ void __launch_bounds__(256) k_bwd_large_rest(DevFronts F, const int32_t* list, int step,
-                                                        const T* __restrict__ panel, const T* V, T* scratch,
-                                                        int nrhs) {
-  __shared__ T part[8][kBwdG][kSolveB];
-  const int f = list[blockIdx.y];
-  const int nc = F.nc[f], nf = nc + F.nr[f];
-  const int c0 = step * kSolveB;
-  if (c0 >= nc) return;
-  const int w = min(kSolveB, nc - c0);
-  const int rs0 = c0 + w;
-  const int rbase = rs0 + blockIdx.x * kSolveRows;
-  if (rbase >= nf) return;
-  const int nchunks = (nf - rs0 + kSolveRows - 1) / kSolveRows;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int i = rbase + warp * 32 + lane;
-  const bool valid = i < nf;
-  const T* P = panel + F.panel_off[f];
-  const T* Vf = V + F.v_off[f] * nrhs;
-  for (int r0 = 0; r0 < nrhs; r0 += kBwdG) {
-    const int g = min(kBwdG, nrhs - r0);
-    T xi[kBwdG];
-#pragma unroll
-    for (int u = 0; u < kBwdG; ++u) xi[u] = (valid && u < g) ? Vf[(int64_t)(r0 + u) * nf + i] : T(0);
-#pragma unroll 1
-    for (int kb = 0; kb < kSolveB; kb += 16) {
-      T pv[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) pv[j] = (valid && kb + j < w) ? P[i + (size_t)(c0 + kb + j) * nf] : T(0);
-#pragma unroll
-      for (int u = 0; u < kBwdG; ++u) {
-        if (u >= g) break;
-        T v[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = pv[j] * xi[u];
-#pragma unroll
-        for (int s = 8; s >= 1; s >>= 1) {
-          const bool up = (lane & s) != 0;
-#pragma unroll
-          for (int j = 0; j < s; ++j) {
-            const T send = up ? v[j] : v[j + s];
-            const T keep = up ? v[j + s] : v[j];
-            v[j] = keep + __shfl_xor_sync(0xffffffffu, send, s);
-          }
-        }
-        v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);   // lanes l and l + 16 hold column kb + (l & 15)
-        if (lane < 16) part[warp][u][kb + lane] = v[0];
-      }
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < g * kSolveB; e += blockDim.x) {
-      const int u = e / kSolveB, k = e % kSolveB;
-      T s = T(0);
-#pragma unroll
-      for (int q = 0; q < 8; ++q) s += part[q][u][k];
-      scratch[F.s_off[f] * nrhs + ((int64_t)(r0 + u) * nchunks + blockIdx.x) * kSolveB + k] = s;
-    }
-    __syncthreads();
-  }
-}
-
-// t_s = v_s - sum over chunks; x_s = Li^T t_s: column i of Li is read by one
-// warp (lanes over k, coalesced; the warp's 16 columns loaded once) and reduced
-// with shuffles
-template <typename T>
-__global__ void __launch_bounds__(256) k_bwd_large_diag(DevFronts F, const int32_t* list, int step,
-                                                        const T* __restrict__ dinv, T* X, int64_t ldx, T* V,
-                                                        const T* scratch, int nrhs) {
-  constexpr int CW = kSolveB / 8;   // columns per warp
-  __shared__ T ts[kSolveB];
-  const int f = list[blockIdx.x];
-  const int nc = F.nc[f], nf = nc + F.nr[f];
-  const int c0 = step * kSolveB;
-  if (c0 >= nc) return;
-  const int w = min(kSolveB, nc - c0);
-  const int rs0 = c0 + w;
-  const int nchunks = nf > rs0 ? (nf - rs0 + kSolveRows - 1) / kSolveRows : 0;
-  const T* Li = inv_block(F, dinv, f, step, blockIdx.x);
-  T* Vf = V + F.v_off[f] * nrhs;
-  const int first = F.first[f];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  T lc[CW][kSolveB / 32];           // Li(lane + 32q, warp*CW + cc); zero above the diagonal
-#pragma unroll
-  for (int cc = 0; cc < CW; ++cc)
-#pragma unroll
-    for (int q = 0; q < kSolveB / 32; ++q) lc[cc][q] = Li[(lane + 32 * q) + (warp * CW + cc) * kSolveB];
-  for (int r = 0; r < nrhs; ++r) {
-    __syncthreads();
-    if (threadIdx.x < kSolveB) {
-      T s = T(0);
-      if (threadIdx.x < w) {
-        s = Vf[(int64_t)r * nf + c0 + threadIdx.x];
-        for (int q = 0; q < nchunks; ++q)
-          s -= scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + q) * kSolveB + threadIdx.x];
-      }
-      ts[threadIdx.x] = s;
-    }
-    __syncthreads();
-    T tv[kSolveB / 32];
-#pragma unroll
-    for (int q = 0; q < kSolveB / 32; ++q) tv[q] = ts[lane + 32 * q];
-#pragma unroll
-    for (int cc = 0; cc < CW; ++cc) {
-      T s = T(0);
-#pragma unroll
-      for (int q = 0; q < kSolveB / 32; ++q) s += lc[cc][q] * tv[q];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      const int i = warp * CW + cc;
-      if (lane == 0 && i < w) {
-        Vf[(int64_t)r * nf + c0 + i] = s;
-        X[first + c0 + i + r * ldx] = s;
-      }
-    }
-  }
-}
+constexpr int kBwdG = 4;   // right-hand sides per pass of the backward partial sums
 
 // ---- fused backward step (one launch per panel step) -------------------------
 // Backward, any number of right-hand sides: every CTA writes its chunk's
-// partial sums; the last CTA of the front to finish (ticket on cnt[slot])
+// partial sums (64 rows; warp (g, q) takes rows 32g .. 32g+31 against the
+// block's columns 32q .. 32q+31, lane = row, coalesced column reads, 16
+// columns at a time, then a butterfly transpose-reduce leaves column kb +
+// (l mod 16)'s sum in lane l); the last CTA of the front to finish (ticket on cnt[slot])
 // sums them in chunk order (deterministic), forms x_s = Li^T t_s, writes V_s
 // and X, and resets the ticket.  A front without rows below the block is
 // finished by CTA 0 alone.
@@ -1733,7 +1616,7 @@ __global__ void __launch_bounds__(256) k_bwd_large_step(DevFronts F, const int32
                                                         T* X, int64_t ldx, T* V, T* scratch, int32_t* cnt,
                                                         int nrhs) {
   constexpr int CW = kSolveB / 8;
-  __shared__ T part[8][kBwdG][kSolveB];
+  __shared__ T part[2][kBwdG][kSolveB];
   __shared__ T ts[kSolveB];
   __shared__ int last;
   const int f = list[blockIdx.y];
@@ -1751,7 +1634,8 @@ __global__ void __launch_bounds__(256) k_bwd_large_step(DevFronts F, const int32
   const T* P = panel + F.panel_off[f];
   T* Vf = V + F.v_off[f] * nrhs;
   if (nchunks > 0) {
-    const int i = rbase + warp * 32 + lane;
+    const int rg = warp & 1, cq = warp >> 1;
+    const int i = rbase + rg * 32 + lane;
     const bool valid = i < nf;
     for (int r0 = 0; r0 < nrhs; r0 += kBwdG) {
       const int g = min(kBwdG, nrhs - r0);
@@ -1759,7 +1643,7 @@ __global__ void __launch_bounds__(256) k_bwd_large_step(DevFronts F, const int32
 #pragma unroll
       for (int u = 0; u < kBwdG; ++u) xi[u] = (valid && u < g) ? Vf[(int64_t)(r0 + u) * nf + i] : T(0);
 #pragma unroll 1
-      for (int kb = 0; kb < kSolveB; kb += 16) {
+      for (int kb = 32 * cq; kb < 32 * cq + 32; kb += 16) {
         T pv[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) pv[j] = (valid && kb + j < w) ? P[i + (size_t)(c0 + kb + j) * nf] : T(0);
@@ -1780,15 +1664,13 @@ __global__ void __launch_bounds__(256) k_bwd_large_step(DevFronts F, const int32
             }
           }
           v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);
-          if (lane < 16) part[warp][u][kb + lane] = v[0];
+          if (lane < 16) part[rg][u][kb + lane] = v[0];
         }
       }
       __syncthreads();
       for (int e = threadIdx.x; e < g * kSolveB; e += blockDim.x) {
         const int u = e / kSolveB, k = e % kSolveB;
-        T s = T(0);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) s += part[q][u][k];
+        const T s = part[0][u][k] + part[1][u][k];
         scratch[F.s_off[f] * nrhs + ((int64_t)(r0 + u) * nchunks + blockIdx.x) * kSolveB + k] = s;
       }
       __syncthreads();
@@ -1814,8 +1696,14 @@ __global__ void __launch_bounds__(256) k_bwd_large_step(DevFronts F, const int32
       T s = T(0);
       if (threadIdx.x < w) {
         s = Vf[(int64_t)r * nf + c0 + threadIdx.x];
-        for (int q = 0; q < nchunks; ++q)      // other CTAs' partials: read past L1
-          s -= __ldcg(&scratch[F.s_off[f] * nrhs + ((int64_t)r * nchunks + q) * kSolveB + threadIdx.x]);
+        const T* pr = scratch + F.s_off[f] * nrhs + (int64_t)r * nchunks * kSolveB + threadIdx.x;
+        for (int q0 = 0; q0 < nchunks; q0 += 8) {   // other CTAs' partials (read past L1), 8 loads in flight,
+          T pv[8];                                   // subtracted in chunk order
+#pragma unroll
+          for (int q = 0; q < 8; ++q) pv[q] = q0 + q < nchunks ? __ldcg(pr + (int64_t)(q0 + q) * kSolveB) : T(0);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) s -= pv[q];
+        }
       }
       ts[threadIdx.x] = s;
     }

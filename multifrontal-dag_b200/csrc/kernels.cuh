@@ -17,8 +17,9 @@ constexpr int kTrRowsH = 64;         // rows per CTA of the panel TRSM
 constexpr int kUpdTile = 128;        // trailing-update output tile (tensor path)
 constexpr int kUpdTileSimt = 64;     // trailing-update output tile (FMA path)
 constexpr int kSolveB = kFactB;      // column step of the large-front solves (one inverted diagonal block)
-constexpr int kSolveRows = 256;      // rows per CTA of the backward large-front partial sums
+constexpr int kSolveRows = 64;       // rows per CTA of the backward large-front partial sums
 constexpr int kMrhsRows = 64;        // rows per CTA of the many-RHS backward partial sums
+static_assert(kSolveRows >= kMrhsRows, "solve scratch is sized for kMrhsRows-row chunks");
 
 #ifdef __CUDACC__
 // Lower tile (ti, tj) of the trailing T x T tile grid (tile width tw) handled by

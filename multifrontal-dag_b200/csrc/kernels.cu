@@ -312,8 +312,11 @@ constexpr int kSfW = 8;   // panel width of the small-front elimination
 // Fused small front: zero, assemble A, extend-add the children in order, partial
 // Cholesky of the nc supernode columns and the Schur complement, all in shared
 // memory; writes the factor panel and the update matrix once.
-template <typename T>
-__global__ void __launch_bounds__(256, 8) k_small_front(DevFronts F, const int32_t* list, const double* __restrict__ a,
+// BIG (fronts of 65..128 rows, the upper levels, few fronts per launch): more
+// registers per thread and the children's update columns loaded 16 at a time
+// per thread; otherwise 8 CTAs per SM and one column per warp step.
+template <typename T, bool BIG>
+__global__ void __launch_bounds__(256, BIG ? 2 : 8) k_small_front(DevFronts F, const int32_t* list, const double* __restrict__ a,
                                                      T* __restrict__ panel, T* __restrict__ upool, int32_t* info) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S = reinterpret_cast<T*>(smem_raw);     // the front's lower triangle, packed by columns
@@ -340,7 +343,8 @@ __global__ void __launch_bounds__(256, 8) k_small_front(DevFronts F, const int32
     const int32_t* loc = F.local + F.lrow_off[c];
     for (int i = tid; i < nrc; i += nt) sloc[i] = loc[i];
     __syncthreads();
-    extend_add_cols(S, -nf, upool + F.u_off[c], sloc, nrc, tid, nt);
+    if constexpr (BIG) extend_add_smem<16>(S, -nf, upool + F.u_off[c], sloc, nrc, tid, nt);
+    else extend_add_cols(S, -nf, upool + F.u_off[c], sloc, nrc, tid, nt);
     __syncthreads();
   }
   // blocked right-looking elimination, panels of kSfW columns, three barriers
@@ -2076,7 +2080,8 @@ void set_smem(KernelT, size_t) {}
 cudaError_t prepare_kernels() {
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t r) { if (r != cudaSuccess && e == cudaSuccess) e = r; };
-  chk(opt_in(k_small_front<double>)); chk(opt_in(k_small_front<float>));
+  chk(opt_in(k_small_front<double, false>)); chk(opt_in(k_small_front<float, false>));
+  chk(opt_in(k_small_front<double, true>)); chk(opt_in(k_small_front<float, true>));
   chk(opt_in(k_trsm2<double>)); chk(opt_in(k_trsm2<float>));
   chk(opt_in(k_update_dmma));
   chk(opt_in(k_potrf<double>)); chk(opt_in(k_potrf<float>));
@@ -2115,8 +2120,8 @@ void launch_small_fronts(const DevFronts& F, const int32_t* list, int count, int
     return;
   }
   size_t sm = small_front_smem<T>(nf_max);
-  set_smem(k_small_front<T>, sm);
-  k_small_front<T><<<count, 256, sm, st>>>(F, list, a, panel, upool, info);
+  if (nf_max > 64) k_small_front<T, true><<<count, 256, sm, st>>>(F, list, a, panel, upool, info);
+  else k_small_front<T, false><<<count, 256, sm, st>>>(F, list, a, panel, upool, info);
 }
 template <typename T>
 void launch_zero_large(const DevFronts& F, const int32_t* list, int count, int64_t max_cols, T* panel, T* upool,

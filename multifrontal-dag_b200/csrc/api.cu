@@ -147,6 +147,11 @@ struct mfd_handle {
   cudaStream_t st2 = nullptr;                       // lookahead: trailing updates off the panel critical path
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // a level's independent launches (small-front size bins) on side streams,
+  // forked from st at the level's start and joined back at its end
+  static constexpr int kSide = 4;
+  cudaStream_t sst[kSide] = {};
+  cudaEvent_t ev_lvl = nullptr, ev_side[kSide] = {};
 
   // systems
   std::vector<Symbolic> sys;
@@ -216,6 +221,11 @@ struct mfd_handle {
     if (ev1) cudaEventDestroy(ev1);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_lvl) cudaEventDestroy(ev_lvl);
+    for (int b = 0; b < kSide; ++b) {
+      if (ev_side[b]) cudaEventDestroy(ev_side[b]);
+      if (sst[b]) cudaStreamDestroy(sst[b]);
+    }
     if (st2) cudaStreamDestroy(st2);
     if (st) cudaStreamDestroy(st);
   }
@@ -679,6 +689,22 @@ cudaEvent_t take_event(mfd_handle* h, size_t idx) {
 }
 
 // Runs `launch` and, when profiling, brackets it with events on the stream.
+// Side streams for one level's small-front bins: fork(k) makes the first k
+// side streams wait for everything queued on st so far; join(k) makes st wait
+// for them.  Concurrency is off in the profiling schedule (every kernel timed
+// alone) and when reserved[4] = 1.
+bool side_streams(const mfd_handle* h) { return !h->profiling && h->opt.reserved[4] != 1; }
+void side_fork(mfd_handle* h, cudaStream_t st, int k) {
+  cudaEventRecord(h->ev_lvl, st);
+  for (int b = 0; b < k; ++b) cudaStreamWaitEvent(h->sst[b], h->ev_lvl, 0);
+}
+void side_join(mfd_handle* h, cudaStream_t st, int k) {
+  for (int b = 0; b < k; ++b) {
+    cudaEventRecord(h->ev_side[b], h->sst[b]);
+    cudaStreamWaitEvent(st, h->ev_side[b], 0);
+  }
+}
+
 template <typename Fn>
 void record(mfd_handle* h, cudaStream_t st, int kind, double flops, double bytes, Fn&& launch) {
   if (!h->profiling) {
@@ -736,16 +762,26 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
   n += 2;
   // trailing update: 0 tensor cores (FP64: DMMA; FP32: tcgen05 3xTF32), 1 FFMA tiles, 2 tcgen05 1xTF32 (FP32)
   const int kind = h->opt.reserved[0];
+  const bool side = side_streams(h);
   for (const LevelPlan& L : h->levels) {
-    for (const LaunchList& s : L.small) {
+    // the level's small-front bins and its large fronts are independent (their
+    // children are on lower levels; their update matrices are distinct blocks)
+    const int nside = side && (L.small.size() > 1 || L.large.count) ? (int)std::min<size_t>(L.small.size(), mfd_handle::kSide) : 0;
+    if (nside) side_fork(h, st, nside);
+    for (size_t b = 0; b < L.small.size(); ++b) {
+      const LaunchList& s = L.small[b];
+      cudaStream_t sb = (int)b < nside ? h->sst[b] : st;
       double fl = 0, by = 0;
       if (prof)
         for (int i = 0; i < s.count; ++i) small_work(h, hl[s.off + i], w, fl, by);
-      record(h, st, MFD_K_SMALL_FRONT, fl, by,
-             [&] { launch_small_fronts<T>(F, lists + s.off, s.count, s.param, a, panel, upool, h->d_info.p, st); });
+      record(h, sb, MFD_K_SMALL_FRONT, fl, by,
+             [&] { launch_small_fronts<T>(F, lists + s.off, s.count, s.param, a, panel, upool, h->d_info.p, sb); });
       ++n;
     }
-    if (L.large.count == 0) continue;
+    if (L.large.count == 0) {
+      if (nside) side_join(h, st, nside);
+      continue;
+    }
     double zb = 0, ab = 0;
     if (prof)
       for (int i = 0; i < L.large.count; ++i) {
@@ -833,6 +869,7 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
       }
     }
     if (pending) cudaStreamWaitEvent(st, h->ev_join, 0);
+    if (nside) side_join(h, st, nside);
   }
   // values of the permuted full matrix for residuals
   record(h, st, MFD_K_OTHER, 0, 0, [&] {
@@ -870,12 +907,23 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       by += w * e + w * nrhs * (2.0 * (f.nc + f.nr) + f.nr);
     }
   };
+  // per level, the small-front bins run on side streams next to the large
+  // fronts (independent: each front reads its children's vectors, on lower
+  // levels in the forward sweep and ancestors' X entries in the backward one)
+  const bool side = side_streams(h);
+  auto nside_of = [&](const LevelPlan& L) {
+    return side && (L.small.size() > 1 || L.large.count) ? (int)std::min<size_t>(L.small.size(), mfd_handle::kSide) : 0;
+  };
   for (const LevelPlan& L : h->levels) {
-    for (const LaunchList& s : L.small) {
+    const int nside = nside_of(L);
+    if (nside) side_fork(h, st, nside);
+    for (size_t b = 0; b < L.small.size(); ++b) {
+      const LaunchList& s = L.small[b];
+      cudaStream_t sb = (int)b < nside ? h->sst[b] : st;
       double fl = 0, by = 0;
       work(s, fl, by);
-      record(h, st, MFD_K_SOLVE_SMALL, fl, by,
-             [&] { launch_fwd_small<T>(F, lists + s.off, s.count, s.param, panel, X, ldx, V, nrhs, st); });
+      record(h, sb, MFD_K_SOLVE_SMALL, fl, by,
+             [&] { launch_fwd_small<T>(F, lists + s.off, s.count, s.param, panel, X, ldx, V, nrhs, sb); });
       ++n;
     }
     if (L.large.count) {
@@ -886,9 +934,21 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
                             ldx, V, h->d_cnt.p, nrhs, st, &n, solve_pdl);
       });
     }
+    if (nside) side_join(h, st, nside);
   }
   for (auto it = h->levels.rbegin(); it != h->levels.rend(); ++it) {
     const LevelPlan& L = *it;
+    const int nside = nside_of(L);
+    if (nside) side_fork(h, st, nside);
+    for (size_t b = 0; b < L.small.size(); ++b) {
+      const LaunchList& s = L.small[b];
+      cudaStream_t sb = (int)b < nside ? h->sst[b] : st;
+      double fl = 0, by = 0;
+      work(s, fl, by);
+      record(h, sb, MFD_K_SOLVE_SMALL, fl, by,
+             [&] { launch_bwd_small<T>(F, lists + s.off, s.count, s.param, panel, X, ldx, nrhs, sb); });
+      ++n;
+    }
     if (L.large.count) {
       double fl = 0, by = 0;
       work(L.large, fl, by);
@@ -897,13 +957,7 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
                             ldx, V, S, h->d_cnt.p, nrhs, st, &n, solve_pdl);
       });
     }
-    for (const LaunchList& s : L.small) {
-      double fl = 0, by = 0;
-      work(s, fl, by);
-      record(h, st, MFD_K_SOLVE_SMALL, fl, by,
-             [&] { launch_bwd_small<T>(F, lists + s.off, s.count, s.param, panel, X, ldx, nrhs, st); });
-      ++n;
-    }
+    if (nside) side_join(h, st, nside);
   }
   return n;
 }
@@ -1123,6 +1177,11 @@ int create_common(mfd_handle** out, std::vector<Symbolic>&& syms, const mfd_opti
   CK(cudaStreamCreateWithPriority(&h->st2, cudaStreamNonBlocking, prio_lo));
   CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h->ev_lvl, cudaEventDisableTiming));
+  for (int b = 0; b < mfd_handle::kSide; ++b) {
+    CK(cudaStreamCreateWithPriority(&h->sst[b], cudaStreamNonBlocking, prio_lo));
+    CK(cudaEventCreateWithFlags(&h->ev_side[b], cudaEventDisableTiming));
+  }
   CK(cudaEventCreate(&h->ev0));
   CK(cudaEventCreate(&h->ev1));
   int rc = build_plan(h.get());

@@ -206,6 +206,30 @@ def test_programmatic_launch_matches():
     assert np.array_equal(x0, x1)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_side_stream_levels_bitwise_equal(precision):
+    """A level's small-front size bins on side streams next to its large
+    fronts (the default) and the same launches on one stream (reserved[4] = 1)
+    touch disjoint data: identical factors and solutions, single and several
+    right-hand sides, on a batch with all four size bins in most levels."""
+    systems = P.laplace2d_batch(12, 5)
+    outs = []
+    for res in ((0, 0, 0, 0, 0, 0, 0), (0, 0, 0, 0, 1, 0, 0)):
+        s = H.Solver.analyze_batch([(q.n, q.col, q.row, q.order) for q in systems], max_zero=100,
+                                   precision=precision, reserved=res)
+        vals = np.concatenate([q.val for q in systems])
+        assert s.factorize(vals) == 0
+        b = np.concatenate([q.rhs for q in systems])
+        x1 = b.copy()
+        s.solve(x1)
+        xm = np.asfortranarray(b[:, None] * np.arange(1, 10)[None, :])
+        s.solve(xm, nrhs=9)
+        outs.append((x1, xm))
+        s.close()
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+
+
 def test_autotune_picks_a_candidate():
     """The autotuner times the schedule candidates and returns options whose
     handle factors to the same solution quality."""

@@ -1287,15 +1287,16 @@ __device__ __forceinline__ void fwd_small_front(const DevFronts& F, int f, const
 #pragma unroll
     for (int q = 0; q < R; ++q) v[q] = vs[lane + 32 * q];
     __syncwarp();
-    // columns in groups of 8 with predicated (not early-exited) steps, so the
+    // columns in groups of G with predicated (not early-exited) steps, so the
     // group's loads issue together: one memory latency per group
+    constexpr int G = 8;
     for (int k0 = 0; k0 < nc; k0 += 32) {
       const int qb = k0 >> 5, kn = min(32, nc - k0);
       const T dk = pick(dinv, qb);
-      for (int g = 0; g < kn; g += 8) {
-        T l[8][R];
+      for (int g = 0; g < kn; g += G) {
+        T l[G][R];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+        for (int u = 0; u < G; ++u) {
           const int k = k0 + g + u;
           const T* Pk = P + (size_t)k * nf;
 #pragma unroll
@@ -1305,7 +1306,7 @@ __device__ __forceinline__ void fwd_small_front(const DevFronts& F, int f, const
           }
         }
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+        for (int u = 0; u < G; ++u) {
           if (g + u < kn) {
             const int kk = g + u, k = k0 + kk;
             const T yk = __shfl_sync(0xffffffffu, pick(v, qb) * dk, kk);
@@ -1354,43 +1355,64 @@ __device__ __forceinline__ void bwd_small_front(const DevFronts& F, int f, const
     __syncwarp();
     for (int b = (nc - 1) >> 5; b >= 0; --b) {
       const int j0 = 32 * b, e = min(j0 + 32, nc), kn = e - j0;   // the block's columns [j0, e)
-      // rows below the triangle [e, nf), lanes over rows, 8 columns at a time:
-      // tile(lane, kk) = sum over the lane's rows i of L(i, j0+kk) x_i
-      for (int g = 0; g < kn; g += 8) {
-        T acc[8];
+      T s = T(0);
+      if constexpr (R == 1) {
+        // nf <= 32: the whole panel in one pass, lanes over rows (one memory
+        // latency): triangle rows raw and lower, rows below nc as products
+        // with x, summed per column in row order
+        const int i = lane;
+        const bool tri = i < nc, ok = i < nf;
+        const T xi = (!tri && ok) ? xs[i] : T(0);
+        T l[32];
 #pragma unroll
-        for (int kk = 0; kk < 8; ++kk) acc[kk] = T(0);
-        for (int i0 = e; i0 < nf; i0 += 32) {
-          const int i = i0 + lane;
-          const bool ok = i < nf;
-          const T xi = ok ? xs[i] : T(0);
-          const T* Pi = P + i + (size_t)(j0 + g) * nf;
-          T l[8];
+        for (int kk = 0; kk < 32; ++kk) l[kk] = (ok && kk < nc && (!tri || kk <= i)) ? P[i + (size_t)kk * nf] : T(0);
 #pragma unroll
-          for (int kk = 0; kk < 8; ++kk) l[kk] = (ok && g + kk < kn) ? Pi[(size_t)kk * nf] : T(0);
+        for (int kk = 0; kk < 32; ++kk) tile[lane * kTileLd + kk] = tri ? l[kk] : l[kk] * xi;
+        __syncwarp();
 #pragma unroll
-          for (int kk = 0; kk < 8; ++kk) acc[kk] += l[kk] * xi;
+        for (int ii = 0; ii < 32; ++ii) {
+          const T v = tile[ii * kTileLd + lane];
+          if (ii >= nc && ii < nf) s += v;
         }
+      } else {
+        // rows below the triangle [e, nf), lanes over rows, 8 columns at a time:
+        // tile(lane, kk) = sum over the lane's rows i of L(i, j0+kk) x_i
+        for (int g = 0; g < kn; g += 8) {
+          T acc[8];
 #pragma unroll
-        for (int kk = 0; kk < 8; ++kk) tile[lane * kTileLd + g + kk] = acc[kk];
-      }
-      __syncwarp();
-      T s = T(0);                                  // columns >= kn of the tile are not written: unused
+          for (int kk = 0; kk < 8; ++kk) acc[kk] = T(0);
+          for (int i0 = e; i0 < nf; i0 += 32) {
+            const int i = i0 + lane;
+            const bool ok = i < nf;
+            const T xi = ok ? xs[i] : T(0);
+            const T* Pi = P + i + (size_t)(j0 + g) * nf;
+            T l[8];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) s += tile[j * kTileLd + lane];
-      __syncwarp();
-      // the triangle, read lanes over rows (row j0 + lane, columns j0 .. row)
-      // into the tile; lane k then reads column k from it
-      {
-        const int i = j0 + lane;
-        const T* Pi = P + i + (size_t)j0 * nf;
+            for (int kk = 0; kk < 8; ++kk) l[kk] = (ok && g + kk < kn) ? Pi[(size_t)kk * nf] : T(0);
 #pragma unroll
-        for (int h = 0; h < 32; h += 16) {
-          T l[16];
+            for (int kk = 0; kk < 8; ++kk) acc[kk] += l[kk] * xi;
+          }
 #pragma unroll
-          for (int kk = 0; kk < 16; ++kk) l[kk] = (h + kk <= lane && lane < kn) ? Pi[(size_t)(h + kk) * nf] : T(0);
+          for (int kk = 0; kk < 8; ++kk) tile[lane * kTileLd + g + kk] = acc[kk];
+        }
+        __syncwarp();
+        // columns >= kn of the tile are not written: unused
 #pragma unroll
-          for (int kk = 0; kk < 16; ++kk) tile[lane * kTileLd + h + kk] = l[kk];
+        for (int j = 0; j < 32; ++j) s += tile[j * kTileLd + lane];
+        __syncwarp();
+        // the triangle, read lanes over rows (row j0 + lane, columns j0 .. row)
+        // into the tile; lane k then reads column k from it
+        {
+          const int i = j0 + lane;
+          const T* Pi = P + i + (size_t)j0 * nf;
+#pragma unroll
+          for (int h = 0; h < 32; h += 16) {
+            T l[16];
+#pragma unroll
+            for (int kk = 0; kk < 16; ++kk) l[kk] = (h + kk <= lane && lane < kn) ? Pi[(size_t)(h + kk) * nf] : T(0);
+#pragma unroll
+            for (int kk = 0; kk < 16; ++kk) tile[lane * kTileLd + h + kk] = l[kk];
+          }
         }
       }
       __syncwarp();

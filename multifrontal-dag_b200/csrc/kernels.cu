@@ -2,13 +2,18 @@
 //
 // Index maps (built once):      local_index, supernodal_index + assembly map,
 //                               block_local_index (reference tiling, export only)
-// Factorization, per tree level: fused one-CTA kernel for small fronts
-//                               (assembly + extend-add + partial Cholesky in
-//                               shared memory); blocked global-memory path for
-//                               large fronts (zero, assemble, extend-add per child
-//                               rank, panel POTRF+TRSM, trailing SYRK/GEMM on the
-//                               FP64 tensor pipe (DMMA) or FFMA tiles)
+// Factorization, per tree level: fused kernels for small fronts (assembly +
+//                               extend-add + partial Cholesky on chip: one warp
+//                               per front up to 32 rows, one CTA per front up to
+//                               128 with the trailing update on DMMA tiles);
+//                               blocked global-memory path for large fronts
+//                               (zero, assemble, extend-add per child rank, panel
+//                               POTRF+TRSM, trailing SYRK/GEMM on the FP64 tensor
+//                               pipe (DMMA), tcgen05 3xTF32 (update_tc.cu) or
+//                               FFMA tiles)
 // Solves:                       forward/backward per level with the same split
+//                               (one warp per small front; 128-column steps with
+//                               the kept inverted diagonal blocks for large ones)
 // Residual / norms:             FP64 CSR SpMV for iterative refinement.
 #include <cuda_runtime.h>
 
@@ -31,12 +36,6 @@ __device__ __forceinline__ int lower_bound_dev(const int32_t* a, int n, int32_t 
   return lo;
 }
 
-template <typename T>
-__device__ __forceinline__ T dev_sqrt(T x);
-template <>
-__device__ __forceinline__ double dev_sqrt<double>(double x) { return sqrt(x); }
-template <>
-__device__ __forceinline__ float dev_sqrt<float>(float x) { return sqrtf(x); }
 
 template <typename T>
 __device__ __forceinline__ T rsqrt_t(T x);

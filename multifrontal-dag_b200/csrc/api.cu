@@ -39,6 +39,7 @@ int fail(int code, const std::string& msg) {
   } while (0)
 
 constexpr int64_t kAlign = 32;  // elements; keeps every front 256-byte aligned in FP64
+constexpr int kResMulti = 4;     // from this many right-hand sides on, one multi-column residual per IR sweep
 int64_t align_up(int64_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 template <typename T>
@@ -186,7 +187,7 @@ struct mfd_handle {
   void* d_panel = nullptr;
   void* d_upool = nullptr;
   void* d_diag = nullptr;
-  DBuf<double> d_a, d_b, d_xp, d_bp, d_r, d_norms, d_cnorms;
+  DBuf<double> d_a, d_b, d_xp, d_bp, d_r, d_norms, d_cnorms, d_xt;
   void* d_X = nullptr;   // T, n_total x nrhs
   void* d_V = nullptr;   // T
   void* d_S = nullptr;   // T
@@ -674,6 +675,7 @@ int ensure_rhs(mfd_handle* h, int nrhs) {
   CK(h->d_bp.alloc((size_t)h->n_total * nrhs));
   CK(h->d_r.alloc((size_t)h->n_total * nrhs));
   CK(h->d_cnorms.alloc((size_t)8 * nrhs));
+  if (h->fp32 && nrhs >= kResMulti) CK(h->d_xt.alloc((size_t)h->n_total * nrhs));
   h->nrhs_cap = nrhs;
   return MFD_OK;
 }
@@ -688,7 +690,6 @@ cudaEvent_t take_event(mfd_handle* h, size_t idx) {
   return h->event_pool[idx];
 }
 
-// Runs `launch` and, when profiling, brackets it with events on the stream.
 // Side streams for one level's small-front bins: fork(k) makes the first k
 // side streams wait for everything queued on st so far; join(k) makes st wait
 // for them.  Concurrency is off in the profiling schedule (every kernel timed
@@ -705,6 +706,7 @@ void side_join(mfd_handle* h, cudaStream_t st, int k) {
   }
 }
 
+// Runs `launch` and, when profiling, brackets it with events on the stream.
 template <typename Fn>
 void record(mfd_handle* h, cudaStream_t st, int kind, double flops, double bytes, Fn&& launch) {
   if (!h->profiling) {
@@ -1102,11 +1104,16 @@ int do_solve(mfd_handle* h, double* b, int nrhs, int64_t ldb, mfd_report* rep) {
       rc = solve_core<float>(h, nrhs);
       if (rc) return rc;
       launch_axpy_from_t<float>(static_cast<float*>(h->d_X), h->d_xp.p, n * nrhs, st);
-      for (int r = 0; r < nrhs; ++r) {
-        const int64_t o = (int64_t)r * n;
-        launch_residual(h->d_csr_ptr.p, h->d_csr_col.p, h->d_csr_val.p, h->d_xp.p + o, h->d_bp.p + o, h->d_r.p + o, n,
-                        st);
-        launch_norms(h->d_r.p + o, h->d_xp.p + o, h->d_bp.p + o, n, h->d_cnorms.p + 8 * r, st);
+      if (nrhs >= kResMulti) {               // A read once for all columns
+        launch_residual_multi(h->d_csr_ptr.p, h->d_csr_col.p, h->d_csr_val.p, h->d_xp.p, h->d_xt.p, h->d_bp.p,
+                              h->d_r.p, n, nrhs, h->d_cnorms.p, st);
+      } else {
+        for (int r = 0; r < nrhs; ++r) {
+          const int64_t o = (int64_t)r * n;
+          launch_residual(h->d_csr_ptr.p, h->d_csr_col.p, h->d_csr_val.p, h->d_xp.p + o, h->d_bp.p + o,
+                          h->d_r.p + o, n, st);
+          launch_norms(h->d_r.p + o, h->d_xp.p + o, h->d_bp.p + o, n, h->d_cnorms.p + 8 * r, st);
+        }
       }
       CK(cudaMemcpyAsync(nv.data(), h->d_cnorms.p, sizeof(double) * 8 * nrhs, cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));

@@ -2030,7 +2030,55 @@ __global__ void k_residual(const int64_t* rowptr, const int32_t* col, const doub
 __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
   atomicMax(reinterpret_cast<unsigned long long*>(addr), __double_as_longlong(v));
 }
+// r = b - A x for k columns at once (x row-major: xt[i * k + c]): one warp per
+// row, lanes over columns (32 at a time), the row's entries loaded 32 at a
+// time and broadcast by shuffles; A is read once for all columns and the
+// lanes' reads of a row of x are contiguous.  Entries are summed in row order,
+// as in k_residual.
+__global__ void k_residual_multi(const int64_t* rowptr, const int32_t* col, const double* val, const double* xt,
+                                 const double* b, double* r, int64_t n, int k) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = w0; i < n; i += nw) {
+    const int64_t e0 = rowptr[i], e1 = rowptr[i + 1];
+    for (int c0 = 0; c0 < k; c0 += 32) {
+      const int c = c0 + lane;
+      double s = 0.0;
+      for (int64_t eb = e0; eb < e1; eb += 32) {
+        const int m = (int)min((int64_t)32, e1 - eb);
+        int cj = 0;
+        double av = 0.0;
+        if (lane < m) {
+          cj = col[eb + lane];
+          av = val[eb + lane];
+        }
+        for (int t = 0; t < m; ++t) {
+          const int j = __shfl_sync(0xffffffffu, cj, t);
+          const double a = __shfl_sync(0xffffffffu, av, t);
+          if (c < k) s += a * xt[(int64_t)j * k + c];
+        }
+      }
+      if (c < k) r[i + (int64_t)c * n] = b[i + (int64_t)c * n] - s;
+    }
+  }
+}
+// column-major n x k (ld n) -> row-major, 32 x 32 tiles through shared memory
+__global__ void k_to_rows(const double* x, double* xt, int64_t n, int k) {
+  __shared__ double t[32][33];
+  const int64_t i0 = (int64_t)blockIdx.x * 32;
+  const int c0 = blockIdx.y * 32, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int c = ty; c < 32; c += 8) t[c][tx] = (i0 + tx < n && c0 + c < k) ? x[i0 + tx + (int64_t)(c0 + c) * n] : 0.0;
+  __syncthreads();
+  for (int q = ty; q < 32; q += 8)
+    if (i0 + q < n && c0 + tx < k) xt[(i0 + q) * k + c0 + tx] = t[tx][q];
+}
+// per column (grid y): out + 8 c gets max|r|, max|x|, max|b|, sum r^2, sum x^2
 __global__ void k_norms(const double* r, const double* x, const double* b, int64_t n, double* out) {
+  r += (int64_t)blockIdx.y * n;
+  x += (int64_t)blockIdx.y * n;
+  b += (int64_t)blockIdx.y * n;
+  out += 8 * blockIdx.y;
   double mr = 0, mx = 0, mb = 0, sr = 0, sx = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double a = fabs(r[i]), c = fabs(x[i]), d = fabs(b[i]);
@@ -2300,6 +2348,14 @@ void launch_residual(const int64_t* rowptr, const int32_t* col, const double* va
 void launch_norms(const double* r, const double* x, const double* b, int64_t n, double* out, cudaStream_t st) {
   cudaMemsetAsync(out, 0, 5 * sizeof(double), st);
   k_norms<<<grid_1d(n), 256, 0, st>>>(r, x, b, n, out);
+}
+void launch_residual_multi(const int64_t* rowptr, const int32_t* col, const double* val, const double* x,
+                           double* xt, const double* b, double* r, int64_t n, int k, double* out, cudaStream_t st) {
+  if (n <= 0 || k <= 0) return;
+  k_to_rows<<<dim3((unsigned)ceil_div(n, 32), (unsigned)ceil_div(k, 32)), 256, 0, st>>>(x, xt, n, k);
+  k_residual_multi<<<grid_1d(n * 32), 256, 0, st>>>(rowptr, col, val, xt, b, r, n, k);
+  cudaMemsetAsync(out, 0, 8 * sizeof(double) * k, st);
+  k_norms<<<dim3(grid_1d(n), k), 256, 0, st>>>(r, x, b, n, out);
 }
 void launch_row_abs_max(const int64_t* rowptr, const double* val, int64_t n, double* out, cudaStream_t st) {
   cudaMemsetAsync(out, 0, sizeof(double), st);

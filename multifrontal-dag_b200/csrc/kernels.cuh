@@ -154,6 +154,10 @@ void launch_residual(const int64_t* rowptr, const int32_t* col, const double* va
                      double* r, int64_t n, cudaStream_t st);
 // out[0]=max|r|, out[1]=max|x|, out[2]=max|b|, out[3]=sum r^2, out[4]=sum x^2 (per column 0 of nrhs)
 void launch_norms(const double* r, const double* x, const double* b, int64_t n, double* out, cudaStream_t st);
+// k columns at once (x column-major, ld n; xt: n x k scratch): r = b - A x and
+// the per-column norms into out + 8 c
+void launch_residual_multi(const int64_t* rowptr, const int32_t* col, const double* val, const double* x,
+                           double* xt, const double* b, double* r, int64_t n, int k, double* out, cudaStream_t st);
 void launch_row_abs_max(const int64_t* rowptr, const double* val, int64_t n, double* out, cudaStream_t st);
 template <typename T>
 void launch_to_t(const double* in, T* out, int64_t n, cudaStream_t st);

@@ -343,17 +343,19 @@ def test_fp32_tensor_update_against_ffma(variant, tol):
     assert rc == 0 and rep.backward_error <= 1e-12
 
 
-def test_fp32_ir_many_rhs():
-    """Block refinement: all right-hand sides refined together, each column
-    to backward error <= 1e-12."""
+@pytest.mark.parametrize("k", [10, 37])
+def test_fp32_ir_many_rhs(k):
+    """Block refinement: all right-hand sides refined together (residuals of
+    all columns in one multi-column SpMV: 37 columns take two 32-lane passes
+    and a partial transpose tile), each column to backward error <= 1e-12."""
     p = P.laplace3d(16)
     s = gpu_for(p, max_zero=1000, precision=H.MFD_PREC_FP32_IR)
     rng = np.random.default_rng(5)
-    B = np.asfortranarray(rng.uniform(-1, 1, (p.n, 10)))
+    B = np.asfortranarray(rng.uniform(-1, 1, (p.n, k)))
     X = B.copy(order="F")
     rep, rc = s.solve(X)
     assert rc == 0 and rep.converged == 1
-    for r in range(10):
+    for r in range(k):
         assert P.backward_error(p.n, p.col, p.row, p.val, X[:, r], B[:, r]) <= 1e-12, r
 
 

@@ -2189,10 +2189,10 @@ void launch_small_fronts(const DevFronts& F, const int32_t* list, int count, int
     return;
   }
   size_t sm = small_front_smem<T>(nf_max);
-  // fronts up to 64 rows: 128 threads per front, so that shared memory (not
-  // the thread count) bounds the fronts in flight per SM (measured faster
-  // than 256 on the 2,000-system batch)
-  if (nf_max > 64) k_small_front<T, true><<<count, 256, sm, st>>>(F, list, a, panel, upool, info);
+  // 128 threads per front, so that shared memory and registers (not the
+  // thread count) bound the fronts in flight per SM (measured faster than 256
+  // on the 2,000-system batch, both variants)
+  if (nf_max > 64) k_small_front<T, true><<<count, 128, sm, st>>>(F, list, a, panel, upool, info);
   else k_small_front<T, false><<<count, 128, sm, st>>>(F, list, a, panel, upool, info);
 }
 template <typename T>

@@ -311,11 +311,13 @@ constexpr int kSfW = 8;   // panel width of the small-front elimination
 // Fused small front: zero, assemble A, extend-add the children in order, partial
 // Cholesky of the nc supernode columns and the Schur complement, all in shared
 // memory; writes the factor panel and the update matrix once.
-// BIG (fronts of 65..128 rows, the upper levels, few fronts per launch): more
-// registers per thread and the children's update columns loaded 16 at a time
-// per thread; otherwise 8 CTAs per SM and one column per warp step.
+// Launched with 128 threads per front.  BIG (fronts of 65..128 rows, the
+// upper levels, few fronts per launch): up to 128 registers per thread and the
+// children's update columns loaded 16 at a time per thread; otherwise 32
+// registers (16 CTAs per SM by registers, shared memory binds first) and one
+// child column per warp step.
 template <typename T, bool BIG>
-__global__ void __launch_bounds__(256, BIG ? 2 : 8) k_small_front(DevFronts F, const int32_t* list, const double* __restrict__ a,
+__global__ void __launch_bounds__(128, BIG ? 4 : 16) k_small_front(DevFronts F, const int32_t* list, const double* __restrict__ a,
                                                      T* __restrict__ panel, T* __restrict__ upool, int32_t* info) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S = reinterpret_cast<T*>(smem_raw);     // the front's lower triangle, packed by columns

@@ -276,6 +276,29 @@ def test_many_rhs_large_fronts(nrhs):
         assert P.backward_error(p.n, p.col, p.row, p.val, X[:, r], B[:, r]) <= FP64_BWD_TOL
 
 
+@pytest.mark.parametrize("sfm", [32, 64, 96, 128])
+@pytest.mark.parametrize("nrhs", [1, 3, 9])
+def test_small_front_bins_against_oracle(sfm, nrhs):
+    """small_front_max 32 .. 128 on a 3D Laplacian with relaxed supernodes
+    routes fronts through every small-front kernel (warp factor, one-CTA
+    factor with 8-column DMMA panels in both size variants, warp-per-front
+    solves with 1..4 row slots, the one-pass backward for nf <= 32) next to
+    the blocked large-front path; one, three (in-kernel RHS loop) and nine
+    (one RHS per CTA row) right-hand sides against the oracle's FP64 solve."""
+    p = P.laplace3d(14)
+    s = gpu_for(p, max_zero=40, small_front_max=sfm)
+    o = oracle_for(p, max_zero=40)
+    rng = np.random.default_rng(sfm + nrhs)
+    B = np.asfortranarray(rng.uniform(-1, 1, (p.n, nrhs)))
+    X = B.copy(order="F")
+    rep, rc = s.solve(X if nrhs > 1 else X[:, 0])
+    assert rc == 0
+    for r in range(nrhs):
+        xo = o.solve(B[:, r])
+        assert np.abs(X[:, r] - xo).max() <= FP64_X_TOL * np.abs(xo).max(), r
+        assert P.backward_error(p.n, p.col, p.row, p.val, X[:, r], B[:, r]) <= FP64_BWD_TOL, r
+
+
 def test_deterministic_replay():
     p = P.laplace3d(12)
     s = gpu_for(p, small_front_max=40)

@@ -391,10 +391,6 @@ int build_plan(mfd_handle* h) {
       for (int32_t g : bins[b]) ll.param2 = std::max(ll.param2, h->fronts[g].nc);   // widest panel of the bin
       L.small.push_back(ll);
     }
-    if (!L.small.empty()) {   // the bins were pushed back to back: one list covers the level
-      L.small_all.off = L.small.front().off;
-      L.small_all.count = L.small.back().off + L.small.back().count - L.small_all.off;
-    }
     if (large.empty()) continue;
     std::stable_sort(large.begin(), large.end(),
                      [&](int32_t a, int32_t b) { return h->fronts[a].nc > h->fronts[b].nc; });

@@ -51,7 +51,6 @@ struct LaunchList {          // a list of front ids in the device list pool
 
 struct LevelPlan {
   std::vector<LaunchList> small;     // fused one-CTA fronts, one list per size bin
-  LaunchList small_all;              // the bins' lists back to back (solves: one launch per level)
   LaunchList large;                  // blocked fronts (sorted by nc descending)
   std::vector<LaunchList> ext_add;   // per child rank: children of large fronts
   std::vector<LaunchList> steps;     // per panel step: prefix of `large`; param = TRSM row blocks,

@@ -388,7 +388,6 @@ int build_plan(mfd_handle* h) {
       ll.off = push_list(h, bins[b]);
       ll.count = (int32_t)bins[b].size();
       ll.param = h->small_bins[b];
-      for (int32_t g : bins[b]) ll.param2 = std::max(ll.param2, h->fronts[g].nc);   // widest panel of the bin
       L.small.push_back(ll);
     }
     if (large.empty()) continue;

@@ -1754,16 +1754,39 @@ __global__ void __launch_bounds__(256, 3) k_bwd_large_step(DevFronts F, const in
 }
 
 // ---- many right-hand sides (nrhs >= kMrhsMin): GEMM-shaped large-front steps --
-// V of a front is an nf x nrhs column-major block (ld nf).  Register-tiled
-// FMA GEMMs over 64-wide RHS tiles; operands stream through shared memory in
-// K chunks of 16 with cp.async double buffering (the next chunk's copies are
-// in flight while the current one is multiplied):
+// V of a front is an nf x nrhs column-major block (ld nf).  GEMMs over 64-wide
+// RHS tiles, on m8n8k4 DMMA in FP64 (one 32 x 32 or 16 x 32 block per warp)
+// and register-tiled FFMA in FP32; operands stream through shared memory in
+// K chunks with cp.async double buffering (the next chunk's copies are in
+// flight while the current one is multiplied):
 //   forward step s : Y = Li V_s (k_mrhs_diag), V_rest -= L_rest,s Y (k_mrhs_fwd_rest)
 //   backward step s: partial(chunk) = L_chunk,s^T X_chunk (k_mrhs_bwd_part, 64-row chunks),
 //                    V_s -= sum of partials in chunk order (k_mrhs_bwd_reduce),
 //                    X_s = Li^T V_s (k_mrhs_diag, transposed)
 constexpr int kMT = 64;          // RHS tile
 constexpr int kMKc = 16;         // K chunk
+
+// FP64: one warp accumulates an (8 MF) x 32 block of C += A B over a K chunk
+// of KC (a multiple of 4) on m8n8k4 DMMA, operands in shared memory as
+// A(i, k) = As[k * lda + i], B(k, j) = Bs[k * ldb + j]; acc[m][n][e] holds
+// C(wr + 8m + g, wc + 8n + 2q + e), g = lane / 4, q = lane % 4
+template <int MF, int KC>
+__device__ __forceinline__ void warp_mma_chunk(double (&acc)[MF][4][2], const double* As, int lda, const double* Bs,
+                                               int ldb, int wr, int wc, int lane) {
+  const int g = lane >> 2, q = lane & 3;
+#pragma unroll
+  for (int k0 = 0; k0 < KC; k0 += 4) {
+    double a[MF], b[4];
+#pragma unroll
+    for (int m = 0; m < MF; ++m) a[m] = As[(k0 + q) * lda + wr + 8 * m + g];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) b[n] = Bs[(k0 + q) * ldb + wc + 8 * n + g];
+#pragma unroll
+    for (int m = 0; m < MF; ++m)
+#pragma unroll
+      for (int n = 0; n < 4; ++n) dmma(acc[m][n][0], acc[m][n][1], a[m], b[n]);
+  }
+}
 
 // Y (128 x 64 RHS tile) = op(Li) V_s, op = identity or transpose; writes V_s and X
 template <typename T>
@@ -1801,6 +1824,10 @@ __global__ void __launch_bounds__(256) k_mrhs_diag(DevFronts F, const int32_t* l
   };
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // rows ty + 16 m (8), RHS tx + 16 n (4)
   T acc[8][4] = {};
+  // FP64: DMMA, warp (warp % 4, warp / 4) owns rows 32 (warp % 4) .. +32, RHS 32 (warp / 4) .. +32
+  double dacc[4][4][2] = {};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wr = 32 * (warp & 3), wc = 32 * (warp >> 2);
   const int nch = (w + KC - 1) / KC;
   load(0, 0);
   for (int c = 0; c < nch; ++c) {
@@ -1812,31 +1839,51 @@ __global__ void __launch_bounds__(256) k_mrhs_diag(DevFronts F, const int32_t* l
     }
     __syncthreads();
     const int b = c & 1;
+    if constexpr (std::is_same<T, double>::value) {
+      warp_mma_chunk<4, KC>(dacc, &As[b][0][0], kSolveB + 4, &Bs[b][0][0], kMT + 4, wr, wc, lane);
+    } else {
 #pragma unroll
-    for (int k = 0; k < KC; ++k) {
-      T a[8], bv[4];
+      for (int k = 0; k < KC; ++k) {
+        T a[8], bv[4];
 #pragma unroll
-      for (int m = 0; m < 8; ++m) a[m] = As[b][k][ty + 16 * m];
+        for (int m = 0; m < 8; ++m) a[m] = As[b][k][ty + 16 * m];
 #pragma unroll
-      for (int n = 0; n < 4; ++n) bv[n] = Bs[b][k][tx + 16 * n];
+        for (int n = 0; n < 4; ++n) bv[n] = Bs[b][k][tx + 16 * n];
 #pragma unroll
-      for (int m = 0; m < 8; ++m)
+        for (int m = 0; m < 8; ++m)
 #pragma unroll
-        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * bv[n];
+          for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * bv[n];
+      }
     }
     __syncthreads();
   }
   const int first = F.first[f];
+  if constexpr (std::is_same<T, double>::value) {
+    const int g = lane >> 2, q = lane & 3;
 #pragma unroll
-  for (int m = 0; m < 8; ++m)
+    for (int m = 0; m < 4; ++m)
 #pragma unroll
-    for (int n = 0; n < 4; ++n) {
-      const int i = ty + 16 * m, r = tx + 16 * n;
-      if (i < w && r < rt) {
-        Vf[(int64_t)(r0 + r) * nf + c0 + i] = acc[m][n];
-        X[first + c0 + i + (int64_t)(r0 + r) * ldx] = acc[m][n];
+      for (int n = 0; n < 4; ++n)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int i = wr + 8 * m + g, r = wc + 8 * n + 2 * q + e;
+          if (i < w && r < rt) {
+            Vf[(int64_t)(r0 + r) * nf + c0 + i] = dacc[m][n][e];
+            X[first + c0 + i + (int64_t)(r0 + r) * ldx] = dacc[m][n][e];
+          }
+        }
+  } else {
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        const int i = ty + 16 * m, r = tx + 16 * n;
+        if (i < w && r < rt) {
+          Vf[(int64_t)(r0 + r) * nf + c0 + i] = acc[m][n];
+          X[first + c0 + i + (int64_t)(r0 + r) * ldx] = acc[m][n];
+        }
       }
-    }
+  }
 }
 
 // V_rest(64-row tile, 64 RHS) -= L(rows, step columns) Y_s
@@ -1872,6 +1919,10 @@ __global__ void __launch_bounds__(256) k_mrhs_fwd_rest(DevFronts F, const int32_
   };
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // rows ty + 16 m (4), RHS tx + 16 n (4)
   T acc[4][4] = {};
+  // FP64: DMMA, warp (warp % 4, warp / 4) owns rows 16 (warp % 4) .. +16, RHS 32 (warp / 4) .. +32
+  double dacc[2][4][2] = {};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wr = 16 * (warp & 3), wc = 32 * (warp >> 2);
   const int nch = (w + kMKc - 1) / kMKc;
   load(0, 0);
   for (int c = 0; c < nch; ++c) {
@@ -1883,27 +1934,44 @@ __global__ void __launch_bounds__(256) k_mrhs_fwd_rest(DevFronts F, const int32_
     }
     __syncthreads();
     const int b = c & 1;
+    if constexpr (std::is_same<T, double>::value) {
+      warp_mma_chunk<2, kMKc>(dacc, &As[b][0][0], kMT + 4, &Bs[b][0][0], kMT + 4, wr, wc, lane);
+    } else {
 #pragma unroll
-    for (int k = 0; k < kMKc; ++k) {
-      T a[4], bv[4];
+      for (int k = 0; k < kMKc; ++k) {
+        T a[4], bv[4];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) a[m] = As[b][k][ty + 16 * m];
+        for (int m = 0; m < 4; ++m) a[m] = As[b][k][ty + 16 * m];
 #pragma unroll
-      for (int n = 0; n < 4; ++n) bv[n] = Bs[b][k][tx + 16 * n];
+        for (int n = 0; n < 4; ++n) bv[n] = Bs[b][k][tx + 16 * n];
 #pragma unroll
-      for (int m = 0; m < 4; ++m)
+        for (int m = 0; m < 4; ++m)
 #pragma unroll
-        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * bv[n];
+          for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * bv[n];
+      }
     }
     __syncthreads();
   }
+  if constexpr (std::is_same<T, double>::value) {
+    const int g = lane >> 2, q = lane & 3;
 #pragma unroll
-  for (int m = 0; m < 4; ++m)
+    for (int m = 0; m < 2; ++m)
 #pragma unroll
-    for (int n = 0; n < 4; ++n) {
-      const int i = i0 + ty + 16 * m, r = tx + 16 * n;
-      if (i < nf && r < rt) Vf[(int64_t)(r0 + r) * nf + i] -= acc[m][n];
-    }
+      for (int n = 0; n < 4; ++n)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int i = i0 + wr + 8 * m + g, r = wc + 8 * n + 2 * q + e;
+          if (i < nf && r < rt) Vf[(int64_t)(r0 + r) * nf + i] -= dacc[m][n][e];
+        }
+  } else {
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        const int i = i0 + ty + 16 * m, r = tx + 16 * n;
+        if (i < nf && r < rt) Vf[(int64_t)(r0 + r) * nf + i] -= acc[m][n];
+      }
+  }
 }
 
 // partial(chunk)(128 columns, 64 RHS) = L(chunk rows, step columns)^T X(chunk rows), 64-row chunks
@@ -1944,6 +2012,10 @@ __global__ void __launch_bounds__(256) k_mrhs_bwd_part(DevFronts F, const int32_
   };
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // columns ty + 16 m (8), RHS tx + 16 n (4)
   T acc[8][4] = {};
+  // FP64: DMMA, warp (warp % 4, warp / 4) owns rows 32 (warp % 4) .. +32, RHS 32 (warp / 4) .. +32
+  double dacc[4][4][2] = {};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wr = 32 * (warp & 3), wc = 32 * (warp >> 2);
   const int nch = (rend - rbase + KC - 1) / KC;
   load(0, rbase);
   for (int c = 0; c < nch; ++c) {
@@ -1955,28 +2027,46 @@ __global__ void __launch_bounds__(256) k_mrhs_bwd_part(DevFronts F, const int32_
     }
     __syncthreads();
     const int b = c & 1;
+    if constexpr (std::is_same<T, double>::value) {
+      warp_mma_chunk<4, KC>(dacc, &As[b][0][0], kSolveB + 4, &Bs[b][0][0], kMT + 4, wr, wc, lane);
+    } else {
 #pragma unroll
-    for (int k = 0; k < KC; ++k) {
-      T a[8], bv[4];
+      for (int k = 0; k < KC; ++k) {
+        T a[8], bv[4];
 #pragma unroll
-      for (int m = 0; m < 8; ++m) a[m] = As[b][k][ty + 16 * m];
+        for (int m = 0; m < 8; ++m) a[m] = As[b][k][ty + 16 * m];
 #pragma unroll
-      for (int n = 0; n < 4; ++n) bv[n] = Bs[b][k][tx + 16 * n];
+        for (int n = 0; n < 4; ++n) bv[n] = Bs[b][k][tx + 16 * n];
 #pragma unroll
-      for (int m = 0; m < 8; ++m)
+        for (int m = 0; m < 8; ++m)
 #pragma unroll
-        for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * bv[n];
+          for (int n = 0; n < 4; ++n) acc[m][n] += a[m] * bv[n];
+      }
     }
     __syncthreads();
   }
+  if constexpr (std::is_same<T, double>::value) {
+    const int g = lane >> 2, q = lane & 3;
 #pragma unroll
-  for (int m = 0; m < 8; ++m)
+    for (int m = 0; m < 4; ++m)
 #pragma unroll
-    for (int n = 0; n < 4; ++n) {
-      const int col = ty + 16 * m, r = tx + 16 * n;
-      if (col < w && r < rt)
-        scratch[F.s_off[f] * nrhs + ((int64_t)(r0 + r) * nchunks + blockIdx.x) * kSolveB + col] = acc[m][n];
-    }
+      for (int n = 0; n < 4; ++n)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int col = wr + 8 * m + g, r = wc + 8 * n + 2 * q + e;
+          if (col < w && r < rt)
+            scratch[F.s_off[f] * nrhs + ((int64_t)(r0 + r) * nchunks + blockIdx.x) * kSolveB + col] = dacc[m][n][e];
+        }
+  } else {
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        const int col = ty + 16 * m, r = tx + 16 * n;
+        if (col < w && r < rt)
+          scratch[F.s_off[f] * nrhs + ((int64_t)(r0 + r) * nchunks + blockIdx.x) * kSolveB + col] = acc[m][n];
+      }
+  }
 }
 
 // V_s(k, r) -= sum over chunks of partial (chunk order), one thread per entry

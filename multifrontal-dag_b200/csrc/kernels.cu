@@ -1527,16 +1527,44 @@ __global__ void __launch_bounds__(256) k_fwd_large_gather(DevFronts F, const int
   T* Vbase = V + F.v_off[f] * nrhs;
   // one right-hand side per CTA when the grid has a y extent (many RHS)
   const int rb = gridDim.y > 1 ? (int)blockIdx.y : 0, re = gridDim.y > 1 ? rb + 1 : nrhs;
+  // loads batched kGU per thread (in flight together); each entry takes one
+  // add per child, children in order
+  constexpr int kGU = 4;
+  const int nt = blockDim.x;
   for (int r = rb; r < re; ++r) {
     T* Vf = Vbase + (int64_t)r * nf;
-    for (int i = threadIdx.x; i < nf; i += blockDim.x) Vf[i] = i < nc ? X[first + i + r * ldx] : T(0);
+    for (int i0 = threadIdx.x; i0 < nf; i0 += kGU * nt) {
+      T xv[kGU];
+#pragma unroll
+      for (int u = 0; u < kGU; ++u) {
+        const int i = i0 + u * nt;
+        xv[u] = i < nc ? X[first + i + r * ldx] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < kGU; ++u)
+        if (i0 + u * nt < nf) Vf[i0 + u * nt] = xv[u];
+    }
     __syncthreads();
     for (int t = F.child_ptr[f]; t < F.child_ptr[f + 1]; ++t) {
       const int c = F.child[t];
       const int ncc = F.nc[c], nrc = F.nr[c];
       const T* Vc = V + F.v_off[c] * nrhs + (int64_t)r * (ncc + nrc) + ncc;
       const int32_t* loc = F.local + F.lrow_off[c];
-      for (int i = threadIdx.x; i < nrc; i += blockDim.x) Vf[loc[i] - 1] += Vc[i];
+      for (int i0 = threadIdx.x; i0 < nrc; i0 += kGU * nt) {
+        int li[kGU];
+        T cv[kGU], ov[kGU];
+#pragma unroll
+        for (int u = 0; u < kGU; ++u) {
+          const int i = i0 + u * nt;
+          li[u] = i < nrc ? loc[i] - 1 : -1;
+          cv[u] = i < nrc ? Vc[i] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < kGU; ++u) ov[u] = li[u] >= 0 ? Vf[li[u]] : T(0);
+#pragma unroll
+        for (int u = 0; u < kGU; ++u)
+          if (li[u] >= 0) Vf[li[u]] = ov[u] + cv[u];
+      }
       __syncthreads();
     }
   }
@@ -1620,9 +1648,24 @@ __global__ void k_bwd_large_gather(DevFronts F, const int32_t* list, const T* X,
   const int nc = F.nc[f], nf = nc + F.nr[f], first = F.first[f];
   const int32_t* lr = F.lrow + F.lrow_off[f];
   const int rb = gridDim.y > 1 ? (int)blockIdx.y : 0, re = gridDim.y > 1 ? rb + 1 : nrhs;
+  constexpr int kGU = 4;                     // loads in flight per thread
+  const int nt = blockDim.x;
   for (int r = rb; r < re; ++r) {
     T* Vf = V + F.v_off[f] * nrhs + (int64_t)r * nf;
-    for (int i = threadIdx.x; i < nf; i += blockDim.x) Vf[i] = i < nc ? X[first + i + r * ldx] : X[lr[i - nc] + r * ldx];
+    for (int i0 = threadIdx.x; i0 < nf; i0 += kGU * nt) {
+      int gi[kGU];
+#pragma unroll
+      for (int u = 0; u < kGU; ++u) {
+        const int i = i0 + u * nt;
+        gi[u] = i < nc ? first + i : (i < nf ? lr[i - nc] : -1);
+      }
+      T xv[kGU];
+#pragma unroll
+      for (int u = 0; u < kGU; ++u) xv[u] = gi[u] >= 0 ? X[gi[u] + r * ldx] : T(0);
+#pragma unroll
+      for (int u = 0; u < kGU; ++u)
+        if (gi[u] >= 0) Vf[i0 + u * nt] = xv[u];
+    }
   }
 }
 

@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 FP64_X_TOL = 1e-10        # ||x - x_oracle||_inf / ||x_oracle||_inf (both FP64, different summation order)
-FP64_BWD_TOL = 1e-12      # normwise backward error
+FP64_BWD_TOL = 1e-12      # normwise backward error target
 FACTOR_TOL = 1e-12        # relative entrywise difference of factor panels
 
 

@@ -149,7 +149,7 @@ int mfd_get_stats(mfd_handle *h, mfd_stats *st);
 /* Autotuner (no counterpart in the reference): times the factorization of the
  * values `a` (host or device pointer, as for mfd_factorize) under candidate
  * settings of the knobs that shape the schedule -- the small-front / blocked
- * split small_front_max in {64, 96, 128, 160} and the lookahead on / off --
+ * split small_front_max in {32, 64, 96, 128} and the lookahead on / off --
  * each on a temporary handle built from h's symbolic data (one warm-up, then
  * the median of `repeats` timed factorizations).  Writes the fastest options
  * to *best and their factor time (ms) to *best_ms; h is left unchanged: create

@@ -1352,7 +1352,7 @@ int mfd_solve(mfd_handle* h, double* b, int32_t nrhs, int64_t ldb, mfd_report* r
 
 int mfd_autotune(mfd_handle* h, const double* a, int32_t repeats, mfd_options* best, double* best_ms) {
   if (!h || !a || !best || repeats < 1) return fail(MFD_E_ARG, "autotune: null handle, values or output");
-  const int sfms[] = {64, 96, 128, 160};
+  const int sfms[] = {32, 64, 96, 128};   // small-front split (at most kSmallFrontMax)
   double best_t = 1e300;
   mfd_options best_o = h->opt;
   for (int sfm : sfms) {

@@ -199,6 +199,15 @@ typedef struct {
 int mfd_set_profiling(mfd_handle *h, int32_t enable);
 int mfd_get_profile(mfd_handle *h, int32_t kind, mfd_kernel_profile *out);
 
+/* Test of the failure path (no counterpart in the reference).  While enabled,
+ * every CTA of the FP32 tensor-core trailing update first waits on an mbarrier
+ * that nothing arrives at, with a ~1 ms limit, before issuing any MMA; the
+ * expired wait raises the handle's error flag and the kernel returns, so the
+ * next mfd_factorize returns MFD_E_TIMEOUT (no GPU fault: every wait is
+ * bounded).  Disable it and the handle factors normally again.  FP64 handles
+ * and fronts that use no tensor-core update are unaffected. */
+int mfd_test_expire_waits(mfd_handle *h, int32_t enable);
+
 int mfd_destroy(mfd_handle *h);
 
 /* ---- dense fronts without allocation ------------------------------------------
@@ -211,7 +220,9 @@ int mfd_destroy(mfd_handle *h);
  * (ld = nf[i], lower triangle used) and an (nf-nc) x (nf-nc) update matrix at
  * update_off[i] (ld = nf-nc; ignored when nf == nc).  On return the panel holds
  * the factor columns and the update matrix has the Schur complement subtracted;
- * *info is 0 or the 1-based front column of the first non-positive pivot.
+ * info points to `count` entries: info[i] is 0, or the 1-based column of front
+ * i where its first non-positive pivot was met (that front's factor is then
+ * not valid; the other fronts are unaffected).
  * Scratch: a static device array of MFD_NOALLOC_MAX_FRONTS x 128 x 128 doubles
  * (1 MiB) plus small tables, held by every GPU that loads the library until the
  * process exits; count > MFD_NOALLOC_MAX_FRONTS is rejected with MFD_E_ARG.

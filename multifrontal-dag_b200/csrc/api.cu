@@ -198,6 +198,7 @@ struct mfd_handle {
       sidx_sys;
 
   bool factored = false;
+  bool expire_waits = false;                        // test request (mfd_test_expire_waits)
   int64_t launches_factor = 0, launches_solve = 0;
   double factor_ms = 0, solve_ms = 0, anorm = 0;
   double time_info[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -489,7 +490,9 @@ int upload_plan(mfd_handle* h) {
   CK(h->d_a_src.alloc(h->nnz_total));
   CK(h->d_a_pos.alloc(h->nnz_total));
   CK(h->d_sidx.alloc(h->nnz_total));
-  CK(h->d_info.alloc(2));   // [0] first bad pivot column, [1] bounded-wait expiry flag
+  // [0] first bad pivot column, [1] bounded-wait expiry flag, [2] test request: make the waits expire
+  CK(h->d_info.alloc(3));
+  CK(cudaMemsetAsync(h->d_info.p, 0, 3 * sizeof(int32_t), h->st));
   CK(h->d_cnt.alloc(std::max(1, h->max_large_count)));   // backward-solve tickets, one per list slot
   CK(cudaMemsetAsync(h->d_cnt.p, 0, sizeof(int32_t) * std::max(1, h->max_large_count), h->st));
   DevFronts& F = h->F;
@@ -996,6 +999,7 @@ int do_factorize(mfd_handle* h, const double* a) {
   CK(cudaSetDevice(h->device));
   cudaMemcpyKind kind = is_device_ptr(a) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   CK(cudaMemcpyAsync(h->d_a.p, a, sizeof(double) * h->nnz_total, kind, h->st));
+  launch_fill_int(h->d_info.p + 2, h->expire_waits ? 1 : 0, 1, h->st);
   CK(cudaEventRecord(h->ev0, h->st));
   int rc = h->fp32 ? run_graph(h, &h->g_factor, [&](cudaStream_t s) { h->launches_factor = enqueue_factor<float>(h, s); })
                    : run_graph(h, &h->g_factor, [&](cudaStream_t s) { h->launches_factor = enqueue_factor<double>(h, s); });
@@ -1472,6 +1476,12 @@ int mfd_set_profiling(mfd_handle* h, int32_t enable) {
   h->profiling = enable != 0;
   std::memset(h->prof, 0, sizeof(h->prof));
   h->pending.clear();
+  return MFD_OK;
+}
+
+int mfd_test_expire_waits(mfd_handle* h, int32_t enable) {
+  if (!h) return fail(MFD_E_ARG, "null handle");
+  h->expire_waits = enable != 0;
   return MFD_OK;
 }
 

@@ -668,9 +668,10 @@ __device__ __forceinline__ T* inv_block(const DevFronts& F, T* linv, int f, int 
   return F.d_off ? linv + F.d_off[f] + (size_t)step * kFactB * kFactB : linv + (size_t)slot * kFactB * kFactB;
 }
 
+// info_stride 0: every front reports into info[0]; 1: list slot i reports into info[i]
 template <typename T>
 __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const int32_t* list, int step, T* panel,
-                                                            T* linv, int32_t* info) {
+                                                            T* linv, int32_t* info, int info_stride) {
   constexpr int B = kFactB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* S = reinterpret_cast<double*>(smem_raw);
@@ -727,7 +728,7 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
     double* Db = Dv + (size_t)b * kPSub * kDLd;
     if (warp == 0) {
       const int bad = warp_chol32(S, o, Db, rq, cbuf, lane);
-      if (bad && lane == 0 && o + bad <= w) atomicMin(info, F.first[f] + c0 + o + bad);
+      if (bad && lane == 0 && o + bad <= w) atomicMin(info + (size_t)info_stride * blockIdx.x, F.first[f] + c0 + o + bad);
     }
     __syncthreads();
     const int rt = nsb - b - 1;                 // 32-row tiles below the sub-block
@@ -2351,9 +2352,10 @@ void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int m
 }
 template <typename T>
 void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
-                  cudaStream_t st, bool pdl) {
+                  cudaStream_t st, bool pdl, int info_stride) {
   if (count <= 0) return;
-  launch_k(k_potrf<T>, dim3(count), dim3(kPotrfThreads), kPotrfSmem, st, pdl, F, list, step, panel, linv, info);
+  launch_k(k_potrf<T>, dim3(count), dim3(kPotrfThreads), kPotrfSmem, st, pdl, F, list, step, panel, linv, info,
+           info_stride);
 }
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
@@ -2516,7 +2518,8 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
   template void launch_assemble_large<T>(const DevFronts&, const int32_t*, int, int, const double*, T*,             \
                                          cudaStream_t);                                                            \
   template void launch_extend_add<T>(const DevFronts&, const int32_t*, int, int, T*, T*, cudaStream_t);             \
-  template void launch_potrf<T>(const DevFronts&, const int32_t*, int, int, T*, T*, int32_t*, cudaStream_t, bool); \
+  template void launch_potrf<T>(const DevFronts&, const int32_t*, int, int, T*, T*, int32_t*, cudaStream_t, bool,  \
+                                int);                                                                              \
   template void launch_trsm<T>(const DevFronts&, const int32_t*, int, int, int, T*, const T*, int, cudaStream_t,   \
                                bool);                                                                              \
   template void launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t,   \

@@ -102,9 +102,10 @@ void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int m
 //            one 128 x 128 slot per list entry when d_off is null)
 //   trsm   : rows below the diagonal block, X <- X L11^{-T}   (kind 0: DMMA, 1: FMA)
 //   update : trailing lower triangle -= P P^T                  (kind 0: DMMA 128-tiles, 1: FMA 64-tiles)
+// info_stride 0: the first bad pivot of any front goes to info[0] (atomic min); 1: list slot i's to info[i]
 template <typename T>
 void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
-                  cudaStream_t st, bool pdl = false);
+                  cudaStream_t st, bool pdl = false, int info_stride = 0);
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
                  const T* linv, int kind, cudaStream_t st, bool pdl = false);
@@ -113,7 +114,8 @@ template <typename T>
 void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, int tiles64, T* panel,
                    T* upool, int kind, cudaStream_t st, int mode = 0, bool pdl = false);
 // FP32 trailing update on the tcgen05 tensor cores (update_tc.cu): split = 1 for 3xTF32, 0 for 1xTF32;
-// err[0] is raised if a bounded wait expires.
+// err[0] is raised if a bounded wait expires; err[1] != 0 (read only) asks every CTA to wait on an
+// mbarrier nothing arrives at, with a short limit, so that err[0] is raised (a test of the expiry path).
 cudaError_t prepare_update_tc();
 void launch_update_tc(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, float* panel,
                       float* upool, int split, int32_t* err, cudaStream_t st, int mode = 0, bool pdl = false);

@@ -92,11 +92,11 @@ extern "C" __attribute__((visibility("default"))) int mfd_factor_fronts_noalloc(
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-  // front tables in the scratch tail: nc, nr, first, list | panel_off, u_off | info
+  // front tables in the scratch tail: nc, nr, first, list | panel_off, u_off | info per front
   struct Tables {
     int32_t nc[kMaxFronts], nr[kMaxFronts], first[kMaxFronts], list[kMaxFronts];
     int64_t poff[kMaxFronts], uoff[kMaxFronts];
-    int32_t info, pad;
+    int32_t info[kMaxFronts];
   } t;
   static_assert(sizeof(Tables) <= kTableWords * sizeof(double), "table area too small");
   std::memset(&t, 0, sizeof(t));
@@ -108,7 +108,7 @@ extern "C" __attribute__((visibility("default"))) int mfd_factor_fronts_noalloc(
     t.poff[i] = panel_off[i];
     t.uoff[i] = update_off[i];
   }
-  t.info = INT_MAX;                                  // the array keeps the last call's contents
+  for (int i = 0; i < kMaxFronts; ++i) t.info[i] = INT_MAX;   // the array keeps the last call's contents
   Tables* dt = reinterpret_cast<Tables*>(scratch + kInvElems);
   cudaError_t e = cudaMemcpyAsync(dt, &t, sizeof(t), cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) { g_msg = cudaGetErrorString(e); return MFD_E_CUDA; }
@@ -120,7 +120,7 @@ extern "C" __attribute__((visibility("default"))) int mfd_factor_fronts_noalloc(
   F.panel_off = dt->poff;
   F.u_off = dt->uoff;
   const int32_t* list = dt->list;
-  int32_t* dinfo = &dt->info;
+  int32_t* dinfo = dt->info;                         // slot i: front i's first bad pivot (list[i] = i)
   const int steps = (maxnc + kFactB - 1) / kFactB;
   for (int s = 0; s < steps; ++s) {
     int rows = 0, tiles = 0;
@@ -133,17 +133,17 @@ extern "C" __attribute__((visibility("default"))) int mfd_factor_fronts_noalloc(
       tiles = T * (T + 1) / 2 > tiles ? T * (T + 1) / 2 : tiles;
     }
     // fronts whose columns are exhausted return at once inside the kernels
-    launch_potrf<double>(F, list, count, s, fronts, scratch, dinfo, st);
+    launch_potrf<double>(F, list, count, s, fronts, scratch, dinfo, st, false, 1);
     launch_trsm<double>(F, list, count, s, rows, fronts, scratch, 0, st);
     launch_update<double>(F, list, count, s, tiles, 0, fronts, fronts, 0, st);
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) { g_msg = cudaGetErrorString(e); return MFD_E_CUDA; }
-  int32_t hinfo = 0;
-  e = cudaMemcpyAsync(&hinfo, dinfo, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  int32_t hinfo[kMaxFronts];
+  e = cudaMemcpyAsync(hinfo, dinfo, sizeof(int32_t) * count, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) { g_msg = cudaGetErrorString(e); return MFD_E_CUDA; }
-  *info = hinfo == INT_MAX ? 0 : hinfo;
+  for (int i = 0; i < count; ++i) info[i] = hinfo[i] == INT_MAX ? 0 : hinfo[i];
   return MFD_OK;
 }
 

@@ -16,7 +16,10 @@
 //     subtracts it from C in place (column-major panel / update matrix, rows
 //     across lanes: coalesced).
 // Every mbarrier wait is bounded (~1 s); on expiry the kernel raises err[0],
-// waits once more (bounded) for its MMAs, frees its tensor memory and returns.
+// waits once more (bounded, ~8 s: MMAs finish in microseconds) for its MMAs,
+// frees its tensor memory and returns.  err[1] != 0 is a test request: before
+// any MMA, every CTA waits on an mbarrier that nothing arrives at, with a
+// ~1 ms limit, so the expiry path runs without any fault.
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -73,7 +76,11 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+constexpr long long kWaitLimit = 1ll << 31;        // cycles (~1.1 s at 1.965 GHz)
+constexpr long long kDrainLimit = 1ll << 34;       // the final wait for issued MMAs
+constexpr long long kProbeLimit = 1ll << 21;       // the test request's wait (~1 ms)
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long long limit = kWaitLimit) {
   const long long t0 = clock64();
   while (true) {
     uint32_t done;
@@ -87,7 +94,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
         : "r"(mbar), "r"(parity)
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > (1ll << 31)) return false;
+    if (clock64() - t0 > limit) return false;
   }
 }
 
@@ -134,12 +141,13 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_update_tc(DevFronts F, const 
   float* U = upool + F.u_off[f];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // 1024-byte aligned stage area, then two mbarriers and the TMEM address slot
+  // 1024-byte aligned stage area, then two mbarriers, the TMEM address slot
+  // and the test request's mbarrier
   const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
   const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
   unsigned char* sm = smem_raw + pad;
   const uint32_t sb = raw + pad;
-  const uint32_t mbar0 = sb + 2 * kStageBytes, mbar1 = mbar0 + 8;
+  const uint32_t mbar0 = sb + 2 * kStageBytes, mbar1 = mbar0 + 8, mbar_probe = mbar0 + 24;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + 2 * kStageBytes + 16);
 
   if (warp == 0) {
@@ -150,6 +158,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_update_tc(DevFronts F, const 
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_probe));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   fence_before_sync();
@@ -162,10 +171,11 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_update_tc(DevFronts F, const 
   const int nch = (w + kTcK - 1) / kTcK;
   bool ok = true;
   int issued = 0;                                   // stages whose MMAs were committed
+  if (err[1]) ok = __syncthreads_and(mbar_wait(mbar_probe, 0, kProbeLimit)) != 0;   // test request: expires
   for (int c = 0; c < nch; ++c) {
     const int buf = c & 1;
     const uint32_t mb = buf ? mbar1 : mbar0;
-    if (c >= 2) ok = __syncthreads_and(mbar_wait(mb, ((c - 2) >> 1) & 1)) != 0;
+    if (c >= 2 && ok) ok = __syncthreads_and(mbar_wait(mb, ((c - 2) >> 1) & 1)) != 0;
     if (!ok) break;
     unsigned char* st = sm + buf * kStageBytes;
     // stage: (row, k-quad) pairs; all global loads first, then split and store
@@ -254,7 +264,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_update_tc(DevFronts F, const 
   } else {
     if (tid == 0) atomicExch(err, 1);
     // MMAs may still be in flight: one more bounded wait for the last commit (it covers all earlier MMAs)
-    if (issued > 0) mbar_wait((issued - 1) & 1 ? mbar1 : mbar0, ((issued - 1) >> 1) & 1);
+    if (issued > 0) mbar_wait((issued - 1) & 1 ? mbar1 : mbar0, ((issued - 1) >> 1) & 1, kDrainLimit);
   }
   fence_before_sync();
   __syncthreads();

@@ -67,7 +67,8 @@ EXPORTS = [
     "mfd_default_options", "mfd_create", "mfd_create_batch", "mfd_analyze", "mfd_analyze_batch", "mfd_factorize",
     "mfd_autotune",
     "mfd_solve", "mfd_factorize_solve", "mfd_get_stats", "mfd_get_index", "mfd_get_symbolic", "mfd_get_front_panel",
-    "mfd_destroy", "mfd_last_error", "mfd_set_profiling", "mfd_get_profile", "mfd_factor_fronts_noalloc",
+    "mfd_destroy", "mfd_last_error", "mfd_set_profiling", "mfd_get_profile", "mfd_test_expire_waits",
+    "mfd_factor_fronts_noalloc",
     "mfd_noalloc_last_error", "mfd_symbolic_analyze", "mfd_symbolic_view", "mfd_symbolic_free", "hppllt_init", "hppllt_set_precision", "hppllt_analyze", "hppllt_set_ordering",
     "hppllt_factorize", "hppllt_solve", "hppllt_finalize", "hppllt_get_time_info", "hppllt_get_cost",
     "hppllt_get_nonzero", "hppllt_get_array_size",
@@ -116,6 +117,7 @@ def load(build_if_missing: bool = True):
     L.mfd_noalloc_last_error.restype = C.c_char_p
     L.mfd_set_profiling.argtypes = [vp, i32]
     L.mfd_get_profile.argtypes = [vp, i32, C.POINTER(KernelProfile)]
+    L.mfd_test_expire_waits.argtypes = [vp, i32]
     L.mfd_symbolic_analyze.argtypes = [C.POINTER(vp), i32, vp, vp, vp, i32]
     L.mfd_symbolic_view.argtypes = [vp, C.POINTER(Symbolic)]
     L.mfd_symbolic_free.argtypes = [vp]
@@ -313,6 +315,10 @@ class Solver:
     def set_profiling(self, enable: bool) -> None:
         _check(load().mfd_set_profiling(self._h, 1 if enable else 0))
 
+    def test_expire_waits(self, enable: bool) -> None:
+        """Make the tensor-core update's first wait run out (mfd_test_expire_waits)."""
+        _check(load().mfd_test_expire_waits(self._h, 1 if enable else 0))
+
     def profile(self) -> dict:
         out = {}
         for k, name in enumerate(KERNEL_CLASSES):
@@ -354,21 +360,26 @@ class Solver:
 NOALLOC_MAX_FRONTS = 8
 
 
-def factor_fronts_noalloc(fronts, panel_off, update_off, nf, nc, stream=None) -> int:
+def factor_fronts_noalloc(fronts, panel_off, update_off, nf, nc, stream=None, per_front=False):
     """Partial Cholesky of dense fronts held in one caller-owned device buffer
     (a float64 CUDA tensor), without any device allocation (see
-    mfd_factor_fronts_noalloc in include/mfdag.h).  Returns info."""
+    mfd_factor_fronts_noalloc in include/mfdag.h).  Returns info: per front
+    (a list, 0 or the front's 1-based bad-pivot column) with per_front=True,
+    else the first nonzero entry of that list (0 if none)."""
     L = load()
     po = np.ascontiguousarray(panel_off, dtype=np.int64)
     uo = np.ascontiguousarray(update_off, dtype=np.int64)
     f = _i32(nf)
     c = _i32(nc)
-    info = np.zeros(1, np.int32)
+    info = np.zeros(max(1, len(f)), np.int32)
     rc = L.mfd_factor_fronts_noalloc(_ptr(fronts), int(len(f)), po.ctypes.data, uo.ctypes.data, f.ctypes.data,
                                      c.ctypes.data, info.ctypes.data, stream)
     if rc != 0:
         raise MfdError(rc, L.mfd_noalloc_last_error().decode())
-    return int(info[0])
+    if per_front:
+        return [int(v) for v in info[:len(f)]]
+    bad = [int(v) for v in info[:len(f)] if v]
+    return bad[0] if bad else 0
 
 
 # index ids of mfd_get_index

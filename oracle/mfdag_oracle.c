@@ -1269,12 +1269,12 @@ EXPORT int orc_factorize(orc_t *h, const double *a) {
   return h->info;
 }
 
-/* hppllt_solve (hppllt.f90:152-173), single RHS in place */
-EXPORT void orc_solve(orc_t *h, double *b) {
+/* hppllt_solve (hppllt.f90:152-173), single RHS in place, with the RHS work
+ * and border arrays of r (h->rh, or a per-thread copy) */
+static void solve_with(orc_t *h, rh_t *r, double *b) {
   int n = h->n;
   double *tmp = xmalloc(sizeof(double) * n);
   for (int i = 0; i < n; i++) tmp[i] = b[h->perm[i] - 1];                        /* permutate */
-  rh_t *r = &h->rh;
   memset(r->work, 0, sizeof(double) * (r->woff[h->num_node] ? r->woff[h->num_node] : 1));
   memset(r->border, 0, sizeof(double) * (r->boff[h->num_node] ? r->boff[h->num_node] : 1));
   r->sup = tmp;
@@ -1291,6 +1291,33 @@ EXPORT void orc_solve(orc_t *h, double *b) {
   for (int i = 0; i < n; i++) b[h->perm[i] - 1] = tmp[i];                        /* inverse_permutate */
   r->sup = NULL;
   free(tmp);
+}
+EXPORT void orc_solve(orc_t *h, double *b) { solve_with(h, &h->rh, b); }
+
+/* Several right-hand sides (column-major, leading dimension ldb), each solved
+ * exactly as orc_solve does, the columns spread over nthreads host threads
+ * with a private RHS work area per thread (the factor is only read). */
+typedef struct { orc_t *h; double *b; int nrhs; int64_t ldb; int next; } many_ctx_t;
+static void *many_worker(void *arg) {
+  many_ctx_t *c = arg;
+  rh_t r;
+  rh_new(&r, &c->h->nd, c->h->node_sets);
+  for (;;) {
+    int k = __atomic_fetch_add(&c->next, 1, __ATOMIC_RELAXED);
+    if (k >= c->nrhs) break;
+    solve_with(c->h, &r, c->b + (int64_t)k * c->ldb);
+  }
+  rh_free(&r);
+  return NULL;
+}
+EXPORT void orc_solve_many(orc_t *h, double *b, int nrhs, int64_t ldb, int nthreads) {
+  many_ctx_t c = {h, b, nrhs, ldb, 0};
+  int nt = nthreads < 1 ? 1 : nthreads > 256 ? 256 : nthreads;
+  if (nt > nrhs) nt = nrhs;
+  pthread_t th[256];
+  for (int i = 1; i < nt; i++) pthread_create(&th[i], NULL, many_worker, &c);
+  many_worker(&c);
+  for (int i = 1; i < nt; i++) pthread_join(th[i], NULL);
 }
 
 /* ------------------------------------------------------------------------- */

@@ -58,6 +58,7 @@ def lib():
     L.orc_factorize_parallel.argtypes = [vp, F64P, C.c_int]
     L.orc_solve.argtypes = [vp, F64P]
     L.orc_sweep.argtypes = [vp, F64P, C.c_int]
+    L.orc_solve_many.argtypes = [vp, F64P, C.c_int, C.c_int64, C.c_int]
     L.orc_get_size.restype = C.c_int
     L.orc_get_size.argtypes = [vp, C.c_int]
     L.orc_get.restype = C.c_int
@@ -231,6 +232,16 @@ class Oracle:
         x = f64(np.array(b, dtype=np.float64, copy=True))
         lib().orc_solve(self._h, x)
         return x
+
+    def solve_many(self, B, nthreads: int = 0) -> np.ndarray:
+        """Solve every column of B (n x k) as solve() does, columns over host threads."""
+        X = np.array(B, dtype=np.float64, order="F", copy=True)
+        if X.ndim == 1:
+            X = X[:, None]
+        flat = X.ravel(order="F")
+        nt = nthreads if nthreads > 0 else (os.cpu_count() or 1)
+        lib().orc_solve_many(self._h, flat, int(X.shape[1]), int(X.shape[0]), int(nt))
+        return flat.reshape(X.shape, order="F")
 
     def sweep(self, permuted_rhs, backward: bool) -> np.ndarray:
         x = f64(np.array(permuted_rhs, dtype=np.float64, copy=True))

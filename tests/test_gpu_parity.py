@@ -425,6 +425,7 @@ def test_hppllt_api_fixture(name):
     assert H.hppllt_get_cost() > 0 and H.hppllt_get_nonzero() > 0
     o = O.Oracle.analyze(n, ptr, row, nb=10, max_zero=10)
     assert H.hppllt_get_cost() == o.cost()
+    assert H.hppllt_get_nonzero() == o.nonzero()           # count_nonzero (cost_calculator_m.f90:22-33)
     for k in (1, 2, 3):
         assert H.hppllt_get_array_size(k) == o.array_size(k)
     H.hppllt_finalize()

@@ -92,3 +92,24 @@ def test_noalloc_partial_fronts_and_limits():
         assert np.abs(u - schur).max() <= 1e-11 * np.abs(schur).max()
     with pytest.raises(H.MfdError):
         H.factor_fronts_noalloc(t, [0] * 9, [0] * 9, [4] * 9, [4] * 9)
+
+
+def test_noalloc_reports_the_failing_front():
+    """Two fronts in one call, the second not positive definite at its column
+    38: the per-front info names that front and column, and the first front's
+    factor is still exact."""
+    import torch
+    nf = nc = 200
+    good = dense_spd(nf, 21)
+    bad = dense_spd(nf, 22)
+    bad[37, 37] = -100.0                                 # pivots 1..37 are unchanged, pivot 38 fails
+    buf = np.concatenate([np.tril(good).ravel(order="F"), np.tril(bad).ravel(order="F")])
+    t = torch.from_numpy(buf.copy()).cuda()
+    info = H.factor_fronts_noalloc(t, [0, nf * nc], [0, 0], [nf, nf], [nc, nc], per_front=True)
+    assert info == [0, 38], info
+    got = np.tril(t.cpu().numpy()[:nf * nc].reshape(nf, nc, order="F"))
+    ref = np.linalg.cholesky(good)
+    assert np.abs(got - ref).max() <= FACTOR_TOL * np.abs(ref).max()
+    # the next call starts from cleared info slots
+    t2 = torch.from_numpy(np.tril(good).ravel(order="F").copy()).cuda()
+    assert H.factor_fronts_noalloc(t2, [0], [0], [nf], [nf], per_front=True) == [0]

@@ -40,6 +40,7 @@ int fail(int code, const std::string& msg) {
 
 constexpr int64_t kAlign = 32;  // elements; keeps every front 256-byte aligned in FP64
 constexpr int kResMulti = 4;     // from this many right-hand sides on, one multi-column residual per IR sweep
+constexpr int kDeferDefault = 2; // panel steps per deferred trailing update (K up to 2 x 128)
 int64_t align_up(int64_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 template <typename T>
@@ -147,6 +148,10 @@ struct mfd_handle {
   cudaStream_t st = nullptr;
   cudaStream_t st2 = nullptr;                       // lookahead: trailing updates off the panel critical path
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // deferred trailing updates: a bulk update on st2 in column bands, one event per band
+  static constexpr int kMaxDefer = 8;
+  cudaEvent_t ev_part[kMaxDefer] = {};
+  int defer = 2;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // a level's independent launches (small-front size bins) on side streams,
   // forked from st at the level's start and joined back at its end
@@ -223,6 +228,8 @@ struct mfd_handle {
     if (ev1) cudaEventDestroy(ev1);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    for (cudaEvent_t e : ev_part)
+      if (e) cudaEventDestroy(e);
     if (ev_lvl) cudaEventDestroy(ev_lvl);
     for (int b = 0; b < kSide; ++b) {
       if (ev_side[b]) cudaEventDestroy(ev_side[b]);
@@ -442,10 +449,8 @@ int build_plan(mfd_handle* h) {
         int w = std::min(kFactB, fr.nc - s * kFactB);
         int nrem = fr.nc + fr.nr - s * kFactB - w;
         rows = std::max(rows, (nrem + kTrRowsH - 1) / kTrRowsH);
-        int T = (nrem + kUpdTile - 1) / kUpdTile;
-        tiles128 = std::max(tiles128, T * (T + 1) / 2);
-        int T6 = (nrem + kUpdTileSimt - 1) / kUpdTileSimt;
-        tiles64 = std::max(tiles64, T6 * (T6 + 1) / 2);
+        tiles128 = std::max(tiles128, (nrem + kUpdTile - 1) / kUpdTile);          // tiles per side
+        tiles64 = std::max(tiles64, (nrem + kUpdTileSimt - 1) / kUpdTileSimt);
       }
       ll.count = cntf;
       ll.param = rows;
@@ -807,68 +812,108 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
       ++n;
     }
     // Lookahead (on unless reserved[1] = 1; profiling runs the serial schedule so
-    // that every kernel is timed alone): after the TRSM of step s, the
-    // update tiles of the next panel's columns run on the main stream and the
-    // rest of the trailing update on the side stream, so POTRF/TRSM of step
-    // s+1 overlap it; the next step's update waits for it (shared columns).
+    // that every kernel is timed alone) with deferred updates (groups of D =
+    // h->defer panel steps, update_k_range): after the TRSM of step s the next
+    // panel's 128 columns take the current group's updates on the main stream
+    // (the catch-up), so POTRF/TRSM of step s+1 can start; at a group's last
+    // step the rest of the trailing matrix takes the whole group's K at once
+    // (the bulk) on the side stream, in column bands: block s+1+k (k < D) first,
+    // each followed by an event, then the rest.  The catch-up of step s+k waits
+    // only for the band it overwrites.  Each tile sees the same K sequence in the
+    // same order as in the serial schedule: bitwise identical results.
     const bool lookahead = h->opt.reserved[1] != 1 && !h->profiling;
     // programmatic dependent launch along the panel chain: opt-in (reserved[2] = 1).
     // Measured on the 64^3 Laplacian it costs 1-2 ms (early-launched CTAs wait on
     // SMs the side-stream update could use), so the default leaves it off.
     const bool pdl = h->opt.reserved[2] == 1 && !h->profiling;
-    bool pending = false;
+    const int D = h->defer;
+    int pend = -1;                            // step of the latest bulk on st2 not yet fully waited for
     for (size_t s = 0; s < L.steps.size(); ++s) {
       const LaunchList& p = L.steps[s];
-      double pf = 0, pb = 0, tf = 0, tb = 0, uf = 0, ub = 0, uf1 = 0, ub1 = 0;
-      if (prof)
+      double pf = 0, pb = 0, tf = 0, tb = 0;
+      bool bulk_any = (s + 1) % D == 0;
+      for (int i = 0; i < p.count; ++i) {
+        const HostFront& f = h->fronts[hl[p.off + i]];
+        if ((f.nc - 1) / kFactB <= (int)s + 1) bulk_any = true;
+        if (!prof) continue;
+        double c0 = (double)s * kFactB, wd = std::min<double>(kFactB, f.nc - c0);
+        double nrem = f.nc + f.nr - c0 - wd;
+        pf += wd * wd * wd / 3 + wd * wd * wd / 3;            // POTRF + triangular inverse
+        pb += w * wd * wd * 2;
+        tf += 2.0 * nrem * wd * wd;                          // X = A Li^T
+        tb += w * (2.0 * nrem * wd + wd * wd);
+      }
+      // algorithmic work of an update launch over a band (update_k_range's rules)
+      auto band_work = [&](UpdBand b, double& fl, double& by) {
+        if (!prof) return;
         for (int i = 0; i < p.count; ++i) {
           const HostFront& f = h->fronts[hl[p.off + i]];
-          double c0 = (double)s * kFactB, wd = std::min<double>(kFactB, f.nc - c0);
-          double nrem = f.nc + f.nr - c0 - wd;
-          pf += wd * wd * wd / 3 + wd * wd * wd / 3;            // POTRF + triangular inverse
-          pb += w * wd * wd * 2;
-          tf += 2.0 * nrem * wd * wd;                          // X = A Li^T
-          tb += w * (2.0 * nrem * wd + wd * wd);
-          uf += 2.0 * wd * nrem * (nrem + 1) / 2;
-          ub += w * (2.0 * nrem * (nrem + 1) / 2 + 2.0 * nrem * wd);
-          double n1 = std::min<double>(nrem, kFactB);          // next-panel columns
-          uf1 += 2.0 * wd * (n1 * (n1 + 1) / 2 + (nrem - n1) * n1);
-          ub1 += w * (2.0 * (n1 * (n1 + 1) / 2 + (nrem - n1) * n1) + 2.0 * nrem * wd);
+          const int last = (f.nc - 1) / kFactB, c0 = (int)s * kFactB, wd = std::min(kFactB, f.nc - c0);
+          const double nrem = f.nc + f.nr - c0 - wd;
+          const int g0 = (int)s >= last ? last : ((int)s / D) * D;
+          const bool bulk = ((int)s + 1) % D == 0 || (int)s >= last - 1;
+          const double K = std::min(f.nc, ((int)s + 1) * kFactB) - g0 * kFactB;
+          for (int blk = b.blo; b.bhi < 0 || blk < b.bhi; ++blk) {
+            const double a0 = (double)blk * kFactB, a1 = std::min(nrem, a0 + kFactB);
+            if (a0 >= nrem) break;
+            if (blk > 0 && !bulk) continue;
+            const double el = (a1 - a0) * nrem - (a0 + a1 - 1) * (a1 - a0) / 2;   // lower-triangle entries
+            fl += 2.0 * K * el;
+            by += w * (2.0 * el + 2.0 * K * (nrem - a0));
+          }
         }
+      };
       record(h, st, MFD_K_PANEL, pf, pb,
              [&] { launch_potrf<T>(F, lists + p.off, p.count, (int)s, panel, diag, h->d_info.p, st, pdl); });
       record(h, st, MFD_K_TRSM, tf, tb, [&] {
         launch_trsm<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, kind == 1 ? 1 : 0, st, pdl);
       });
       n += 2;
-      auto update = [&](cudaStream_t us, int mode) {
+      auto update = [&](cudaStream_t us, UpdBand band) {
+        double fl = 0, by = 0;
+        band_work(band, fl, by);
         const bool upd_pdl = pdl && us == st;        // right behind the TRSM on the main stream
-        if constexpr (sizeof(T) == 4) {
-          if (kind == 0 || kind == 2) {
-            launch_update_tc(F, lists + p.off, p.count, (int)s, p.param2, reinterpret_cast<float*>(panel),
-                             reinterpret_cast<float*>(upool), kind == 0 ? 1 : 0, h->d_info.p + 1, us, mode, upd_pdl);
-            return;
+        record(h, us, MFD_K_UPDATE, fl, by, [&] {
+          if constexpr (sizeof(T) == 4) {
+            if (kind == 0 || kind == 2) {
+              n += launch_update_tc(F, lists + p.off, p.count, (int)s, p.param2, reinterpret_cast<float*>(panel),
+                                    reinterpret_cast<float*>(upool), kind == 0 ? 1 : 0, h->d_info.p + 1, us, band,
+                                    D, upd_pdl);
+              return;
+            }
           }
-        }
-        launch_update<T>(F, lists + p.off, p.count, (int)s, p.param2, p.param3, panel, upool, kind == 1 ? 1 : 0, us,
-                         mode, upd_pdl && kind != 1);
+          n += launch_update<T>(F, lists + p.off, p.count, (int)s, p.param2, p.param3, panel, upool,
+                                kind == 1 ? 1 : 0, us, band, D, upd_pdl && kind != 1);
+        });
       };
-      if (pending) cudaStreamWaitEvent(st, h->ev_join, 0);
-      pending = false;
-      if (lookahead && s + 1 < L.steps.size()) {
+      if (!lookahead || s + 1 == L.steps.size()) {
+        if (pend >= 0) cudaStreamWaitEvent(st, h->ev_join, 0);
+        pend = -1;
+        update(st, UpdBand{0, -1});
+        continue;
+      }
+      if (pend >= 0) {                       // the band of the pending bulk that holds block column s+1
+        const int k = (int)s - pend;
+        if (k >= D) {
+          cudaStreamWaitEvent(st, h->ev_join, 0);
+          pend = -1;
+        } else {
+          cudaStreamWaitEvent(st, h->ev_part[k], 0);
+        }
+      }
+      update(st, UpdBand{0, 1});             // catch-up: the next panel's columns
+      if (bulk_any) {
         cudaEventRecord(h->ev_fork, st);
         cudaStreamWaitEvent(h->st2, h->ev_fork, 0);
-        record(h, h->st2, MFD_K_UPDATE, uf - uf1, ub - ub1, [&] { update(h->st2, 2); });
-        record(h, st, MFD_K_UPDATE, uf1, ub1, [&] { update(st, 1); });
+        for (int k = 1; k < D; ++k) {
+          update(h->st2, UpdBand{k, k + 1});
+          cudaEventRecord(h->ev_part[k], h->st2);
+        }
+        update(h->st2, UpdBand{D, -1});
         cudaEventRecord(h->ev_join, h->st2);
-        pending = true;
-        n += 2;
-      } else {
-        record(h, st, MFD_K_UPDATE, uf, ub, [&] { update(st, 0); });
-        ++n;
+        pend = (int)s;
       }
     }
-    if (pending) cudaStreamWaitEvent(st, h->ev_join, 0);
     if (nside) side_join(h, st, nside);
   }
   // values of the permuted full matrix for residuals
@@ -1183,6 +1228,9 @@ int create_common(mfd_handle** out, std::vector<Symbolic>&& syms, const mfd_opti
   CK(cudaStreamCreateWithPriority(&h->st2, cudaStreamNonBlocking, prio_lo));
   CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+  for (int k = 0; k < mfd_handle::kMaxDefer; ++k) CK(cudaEventCreateWithFlags(&h->ev_part[k], cudaEventDisableTiming));
+  // deferred updates: reserved[5] = group size (1 = none); 0 = default
+  h->defer = h->opt.reserved[5] > 0 ? std::min(h->opt.reserved[5], mfd_handle::kMaxDefer) : kDeferDefault;
   CK(cudaEventCreateWithFlags(&h->ev_lvl, cudaEventDisableTiming));
   for (int b = 0; b < mfd_handle::kSide; ++b) {
     CK(cudaStreamCreateWithPriority(&h->sst[b], cudaStreamNonBlocking, prio_lo));

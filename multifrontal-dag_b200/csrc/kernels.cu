@@ -814,8 +814,9 @@ __device__ __forceinline__ T* trailing_addr(T* P, T* U, int nc, int nr, int nf, 
 }
 
 // Trailing update on the FP64 tensor pipe: one 128x128 tile of the trailing
-// lower triangle per CTA, C -= P_i P_j^T over K = w <= 128 in chunks of 32,
-// double-buffered with cp.async.  16 warps as 4 (rows) x 4 (columns) of 32x32,
+// lower triangle per CTA, C -= P_i P_j^T over the K range of the step's
+// deferred group (update_k_range: up to defer x 128 panel columns) in chunks
+// of 32, double-buffered with cp.async.  16 warps as 4 (rows) x 4 (columns) of 32x32,
 // each 2 x 4 mma.m16n8k16.f64 per K step of 16.  Shared-memory operands are
 // k-major with a row stride of 132 doubles (= 4 mod 16): every fragment load of
 // a half-warp hits 16 distinct 8-byte bank pairs.  The accumulators are loaded
@@ -931,7 +932,7 @@ __global__ void __launch_bounds__(256) k_trsm2(DevFronts F, const int32_t* list,
 }
 
 __global__ void __launch_bounds__(kUThreads, 1) k_update_dmma(DevFronts F, const int32_t* list, int step, double* panel,
-                                                        double* upool, int mode) {
+                                                        double* upool, int blo, int bhi, int defer) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* sm = reinterpret_cast<double*>(smem_raw);     // [stage][operand][k][row]
   const int f = list[blockIdx.y];
@@ -943,12 +944,14 @@ __global__ void __launch_bounds__(kUThreads, 1) k_update_dmma(DevFronts F, const
   const int nrem = nf - base;
   if (nrem <= 0) return;
   const int T = (nrem + kUT - 1) / kUT;
-  int ti, tj;
-  if (!select_tile(mode, T, kUT, blockIdx.x, ti, tj)) return;
+  int ti, tj, kbeg, kend;
+  if (!select_tile(T, kUT, blo, bhi, blockIdx.x, ti, tj)) return;
+  if (!update_k_range(nc, step, defer, tj, kUT, kbeg, kend)) return;
+  const int K = kend - kbeg;                            // panel columns [kbeg, kend) of the front
   const int i0 = base + ti * kUT, j0 = base + tj * kUT;
   double* P = panel + F.panel_off[f];
   double* U = upool + F.u_off[f];
-  const int nchunks = (w + kUK - 1) / kUK;
+  const int nchunks = (K + kUK - 1) / kUK;
   const bool diag = ti == tj;
   auto load = [&](int stage, int kc) {
     double* dst = sm + stage * (2 * kUK * kULD);
@@ -957,8 +960,8 @@ __global__ void __launch_bounds__(kUThreads, 1) k_update_dmma(DevFronts F, const
       const int op = e / (kUK * kUT), rem = e - op * (kUK * kUT);
       const int k = rem / kUT, r = rem - k * kUT;
       const int row = (op == 0 ? i0 : j0) + r, col = kc * kUK + k;
-      const bool valid = row < nf && col < w;
-      const double* src = valid ? P + row + (size_t)(c0 + col) * nf : P;
+      const bool valid = row < nf && col < K;
+      const double* src = valid ? P + row + (size_t)(kbeg + col) * nf : P;
       cp_async8(dst + op * (kUK * kULD) + k * kULD + r, src, valid);
     }
     cp_async_commit();
@@ -1028,7 +1031,7 @@ __global__ void __launch_bounds__(kUThreads, 1) k_update_dmma(DevFronts F, const
 constexpr int kSimtTile = 64, kSimtK = 64;
 template <typename T>
 __global__ void __launch_bounds__(256) k_update_simt(DevFronts F, const int32_t* list, int step, T* panel, T* upool,
-                                                     int mode) {
+                                                     int blo, int bhi, int defer) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int LDK = kSimtTile + 4;
   T* As = reinterpret_cast<T*>(smem_raw);
@@ -1042,8 +1045,10 @@ __global__ void __launch_bounds__(256) k_update_simt(DevFronts F, const int32_t*
   const int nrem = nf - base;
   if (nrem <= 0) return;
   const int Tn = (nrem + kSimtTile - 1) / kSimtTile;
-  int ti, tj;
-  if (!select_tile(mode, Tn, kSimtTile, blockIdx.x, ti, tj)) return;
+  int ti, tj, kbeg, kend;
+  if (!select_tile(Tn, kSimtTile, blo, bhi, blockIdx.x, ti, tj)) return;
+  if (!update_k_range(nc, step, defer, tj, kSimtTile, kbeg, kend)) return;
+  const int K = kend - kbeg;
   const int i0 = base + ti * kSimtTile, j0 = base + tj * kSimtTile;
   T* P = panel + F.panel_off[f];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -1052,15 +1057,15 @@ __global__ void __launch_bounds__(256) k_update_simt(DevFronts F, const int32_t*
   for (int m = 0; m < 4; ++m)
 #pragma unroll
     for (int n = 0; n < 4; ++n) acc[m][n] = T(0);
-  for (int k0 = 0; k0 < w; k0 += kSimtK) {
-    const int kw = min(kSimtK, w - k0);
+  for (int k0 = 0; k0 < K; k0 += kSimtK) {
+    const int kw = min(kSimtK, K - k0);
     __syncthreads();
     batched_loop(
         2 * kSimtTile * kw,
         [&](int e) {
           const int op = e / (kSimtTile * kw), rem = e - op * (kSimtTile * kw);
           const int k = rem / kSimtTile, g = (op ? j0 : i0) + rem % kSimtTile;
-          return g < nf ? P[g + (size_t)(c0 + k0 + k) * nf] : T(0);
+          return g < nf ? P[g + (size_t)(kbeg + k0 + k) * nf] : T(0);
         },
         [&](int e, T v) {
           const int op = e / (kSimtTile * kw), rem = e - op * (kSimtTile * kw);
@@ -2366,31 +2371,32 @@ void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, i
   dim3 grid(row_blocks * 2, count);
   launch_k(k_trsm2<T>, grid, dim3(256), trsm2_smem<T>(), st, pdl, F, list, step, panel, linv);
 }
-int update_grid(int tiles, int tw, int mode) {
-  if (mode != 1) return tiles;
-  int T = 0;
-  while ((T + 1) * (T + 2) / 2 <= tiles) ++T;      // tiles = T (T + 1) / 2
-  return T * (kFactB / tw);
+int update_grid(int T, int tw, UpdBand band) {
+  const int c1 = kFactB / tw, jlo = band.blo * c1;
+  if (T <= 0 || jlo >= T) return 0;
+  if (band.bhi < 0) return (T - jlo) * (T - jlo + 1) / 2;
+  return (T - jlo) * ((band.bhi - band.blo) * c1);
 }
 
 template <typename T>
-void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, int tiles64, T* panel,
-                   T* upool, int kind, cudaStream_t st, int mode, bool pdl) {
-  if (count <= 0) return;
+int launch_update(const DevFronts& F, const int32_t* list, int count, int step, int T128, int T64, T* panel,
+                  T* upool, int kind, cudaStream_t st, UpdBand band, int defer, bool pdl) {
+  if (count <= 0) return 0;
   if constexpr (sizeof(T) == 8) {
     if (kind == 0) {
-      const int g = update_grid(tiles128, kUT, mode);
-      if (g <= 0) return;
+      const int g = update_grid(T128, kUT, band);
+      if (g <= 0) return 0;
       size_t sm = 2 * 2 * (size_t)kUK * kULD * sizeof(double);
       launch_k(k_update_dmma, dim3(g, count), dim3(kUThreads), sm, st, pdl, F, list, step, reinterpret_cast<double*>(panel),
-               reinterpret_cast<double*>(upool), mode);
-      return;
+               reinterpret_cast<double*>(upool), band.blo, band.bhi, defer);
+      return 1;
     }
   }
-  const int g = update_grid(tiles64, kSimtTile, mode);
-  if (g <= 0) return;
+  const int g = update_grid(T64, kSimtTile, band);
+  if (g <= 0) return 0;
   size_t sm = 2 * (size_t)kSimtK * (kSimtTile + 4) * sizeof(T);
-  k_update_simt<T><<<dim3(g, count), 256, sm, st>>>(F, list, step, panel, upool, mode);
+  k_update_simt<T><<<dim3(g, count), 256, sm, st>>>(F, list, step, panel, upool, band.blo, band.bhi, defer);
+  return 1;
 }
 
 // one launch per size bin (nf_max <= 32 R, R <= kSmallFrontMax / 32 = 4)
@@ -2522,8 +2528,8 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
                                 int);                                                                              \
   template void launch_trsm<T>(const DevFronts&, const int32_t*, int, int, int, T*, const T*, int, cudaStream_t,   \
                                bool);                                                                              \
-  template void launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t,   \
-                                 int, bool);                                                                       \
+  template int launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t,    \
+                                 UpdBand, int, bool);                                                              \
   template void launch_fwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, T*, int,    \
                                     cudaStream_t);                                                                 \
   template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, int,         \

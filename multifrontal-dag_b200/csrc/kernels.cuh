@@ -21,26 +21,59 @@ constexpr int kSolveRows = 64;       // rows per CTA of the backward large-front
 constexpr int kMrhsRows = 64;        // rows per CTA of the many-RHS backward partial sums
 static_assert(kSolveRows >= kMrhsRows, "solve scratch is sized for kMrhsRows-row chunks");
 
+// Trailing-update work of panel step s of a front (columns c0 = s * kFactB
+// .. c0 + w, base = c0 + w): the lower triangle of the trailing matrix (rows
+// and columns >= base) in T x T tiles of width tw.  A launch covers one band
+// of tile columns, given in 128-column blocks relative to base: block b holds
+// tile columns [b c1, (b + 1) c1) with c1 = kFactB / tw; bhi < 0 means "to the
+// end".  Block 0 is the next panel's columns.
+//
+// Deferred updates: the panel steps are taken in groups of `defer` (a group
+// also ends at the front's last step and at the step before it, so the last,
+// possibly partial, panel starts a group of its own).  Block 0 takes, at every
+// step, the updates of the current group's steps so far (K range [g0 kFactB,
+// base)); the other blocks take the whole group at once at its last step, and
+// nothing at the others.  Every tile thus receives the same K sequence in the
+// same order as with defer = 1, in fewer passes over C.
 #ifdef __CUDACC__
-// Lower tile (ti, tj) of the trailing T x T tile grid (tile width tw) handled by
-// CTA x of an update launch.  mode 0: every lower tile (x enumerates the
-// triangle row by row); mode 1: only the tiles whose columns belong to the
-// next panel (the first kFactB columns: x = ti * (kFactB / tw) + tj); mode 2:
-// every other tile (x enumerates the triangle; next-panel tiles return).
-__device__ __forceinline__ bool select_tile(int mode, int T, int tw, int x, int& ti, int& tj) {
-  const int c1 = kFactB / tw;
-  if (mode == 1) {
-    ti = x / c1;
-    tj = x - ti * c1;
-    return ti < T && tj <= ti;
+__device__ __forceinline__ int update_grid_dev(int T, int tw, int blo, int bhi) {
+  const int c1 = kFactB / tw, jlo = blo * c1;
+  if (jlo >= T) return 0;
+  if (bhi < 0) {
+    const int t = T - jlo;
+    return t * (t + 1) / 2;
   }
-  if (x >= T * (T + 1) / 2) return false;
-  int i = (int)((sqrtf(8.0f * (float)x + 1.0f) - 1.0f) * 0.5f);
-  while ((i + 1) * (i + 2) / 2 <= x) ++i;
-  while (i * (i + 1) / 2 > x) --i;
-  ti = i;
-  tj = x - i * (i + 1) / 2;
-  return mode == 0 || tj >= c1;
+  return (T - jlo) * ((bhi - blo) * c1);
+}
+// Tile (ti, tj) handled by CTA x of a launch over band [blo, bhi).
+__device__ __forceinline__ bool select_tile(int T, int tw, int blo, int bhi, int x, int& ti, int& tj) {
+  const int c1 = kFactB / tw, jlo = blo * c1;
+  if (jlo >= T) return false;
+  if (bhi < 0) {                              // the sub-triangle of tile columns >= jlo, row by row
+    const int t = T - jlo;
+    if (x >= t * (t + 1) / 2) return false;
+    int i = (int)((sqrtf(8.0f * (float)x + 1.0f) - 1.0f) * 0.5f);
+    while ((i + 1) * (i + 2) / 2 <= x) ++i;
+    while (i * (i + 1) / 2 > x) --i;
+    ti = jlo + i;
+    tj = jlo + (x - i * (i + 1) / 2);
+    return true;
+  }
+  const int wdt = (bhi - blo) * c1;
+  ti = jlo + x / wdt;
+  tj = jlo + x % wdt;
+  return ti < T && tj <= ti;
+}
+// K range [kbeg, kend) (front columns) that tile column tj of step `step`
+// applies; false: nothing to apply at this step.
+__device__ __forceinline__ bool update_k_range(int nc, int step, int defer, int tj, int tw, int& kbeg, int& kend) {
+  const int last = (nc - 1) / kFactB;
+  const int g0 = step >= last ? last : (step / defer) * defer;
+  const bool bulk = (step + 1) % defer == 0 || step >= last - 1;
+  if (tj * tw >= kFactB && !bulk) return false;
+  kbeg = g0 * kFactB;
+  kend = min(nc, (step + 1) * kFactB);
+  return true;
 }
 #endif
 
@@ -109,18 +142,25 @@ void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, 
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
                  const T* linv, int kind, cudaStream_t st, bool pdl = false);
-// Update tile subsets (select_tile): mode 0 all, 1 the next panel's columns, 2 the rest.
+// Trailing update of step `step` over the tile-column band [blo, bhi) (128-column blocks relative to
+// the trailing matrix, bhi < 0: to the end; see select_tile) with updates deferred over groups of
+// `defer` steps (update_k_range).  T128 / T64: the largest front's trailing tiles per side.
+struct UpdBand {
+  int blo = 0, bhi = -1;
+};
+// Returns the number of kernels launched (0 when the band is empty).
 template <typename T>
-void launch_update(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, int tiles64, T* panel,
-                   T* upool, int kind, cudaStream_t st, int mode = 0, bool pdl = false);
+int launch_update(const DevFronts& F, const int32_t* list, int count, int step, int T128, int T64, T* panel,
+                  T* upool, int kind, cudaStream_t st, UpdBand band = {}, int defer = 1, bool pdl = false);
 // FP32 trailing update on the tcgen05 tensor cores (update_tc.cu): split = 1 for 3xTF32, 0 for 1xTF32;
 // err[0] is raised if a bounded wait expires; err[1] != 0 (read only) asks every CTA to wait on an
 // mbarrier nothing arrives at, with a short limit, so that err[0] is raised (a test of the expiry path).
 cudaError_t prepare_update_tc();
-void launch_update_tc(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, float* panel,
-                      float* upool, int split, int32_t* err, cudaStream_t st, int mode = 0, bool pdl = false);
-// grid size of an update launch over `tiles` lower tiles of width tw in the given mode
-int update_grid(int tiles, int tw, int mode);
+int launch_update_tc(const DevFronts& F, const int32_t* list, int count, int step, int T128, float* panel,
+                     float* upool, int split, int32_t* err, cudaStream_t st, UpdBand band = {}, int defer = 1,
+                     bool pdl = false);
+// grid size of an update launch over a band of the T x T lower tiles of width tw
+int update_grid(int T, int tw, UpdBand band);
 
 // ---- solves --------------------------------------------------------------------
 // Small fronts (one size bin, nf <= nf_max <= kSmallFrontMax): one warp per front.

@@ -123,14 +123,14 @@ extern "C" __attribute__((visibility("default"))) int mfd_factor_fronts_noalloc(
   int32_t* dinfo = dt->info;                         // slot i: front i's first bad pivot (list[i] = i)
   const int steps = (maxnc + kFactB - 1) / kFactB;
   for (int s = 0; s < steps; ++s) {
-    int rows = 0, tiles = 0;
+    int rows = 0, tiles = 0;                         // TRSM row blocks, update tiles per side
     for (int i = 0; i < count; ++i) {
       if (nc[i] <= s * kFactB) continue;
       int w = nc[i] - s * kFactB < kFactB ? nc[i] - s * kFactB : kFactB;
       int nrem = nf[i] - s * kFactB - w;
       int rb = (nrem + kTrRowsH - 1) / kTrRowsH, T = (nrem + kUpdTile - 1) / kUpdTile;
       rows = rb > rows ? rb : rows;
-      tiles = T * (T + 1) / 2 > tiles ? T * (T + 1) / 2 : tiles;
+      tiles = T > tiles ? T : tiles;
     }
     // fronts whose columns are exhausted return at once inside the kernels
     launch_potrf<double>(F, list, count, s, fronts, scratch, dinfo, st, false, 1);

@@ -1,7 +1,8 @@
 // Trailing update of the FP32 factorization on the 5th-generation tensor cores.
 //
 // One CTA per 128 x 128 tile of the trailing lower triangle of a front,
-// C -= P_i P_j^T with P the solved panel rows and K = w <= 128:
+// C -= P_i P_j^T with P the solved panel rows over the K range of the step's
+// deferred group (update_k_range: up to defer x 128 columns):
 //   * operands are staged by all 256 threads from the panel (global) into
 //     shared memory in the canonical K-major, no-swizzle UMMA layout
 //     (8-row x 16-byte core matrices), split into TF32 hi / lo parts;
@@ -122,7 +123,7 @@ __device__ __forceinline__ float tf32_hi(float x) {
 
 __global__ void __launch_bounds__(kTcThreads, 2) k_update_tc(DevFronts F, const int32_t* list, int step,
                                                              float* panel, float* upool, int split, int32_t* err,
-                                                             int mode) {
+                                                             int blo, int bhi, int defer) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const int f = list[blockIdx.y];
   const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
@@ -133,8 +134,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_update_tc(DevFronts F, const 
   const int nrem = nf - base;
   if (nrem <= 0) return;
   const int T = (nrem + kTcTile - 1) / kTcTile;
-  int ti, tj;
-  if (!select_tile(mode, T, kTcTile, blockIdx.x, ti, tj)) return;
+  int ti, tj, kbeg, kend;
+  if (!select_tile(T, kTcTile, blo, bhi, blockIdx.x, ti, tj)) return;
+  if (!update_k_range(nc, step, defer, tj, kTcTile, kbeg, kend)) return;
+  const int K = kend - kbeg;                        // panel columns [kbeg, kend) of the front
   const int i0 = base + ti * kTcTile, j0 = base + tj * kTcTile;
   const bool diag = ti == tj;
   float* P = panel + F.panel_off[f];
@@ -168,7 +171,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_update_tc(DevFronts F, const 
   pdl_wait();                       // the panel rows are the preceding TRSM's output
   pdl_trigger();
 
-  const int nch = (w + kTcK - 1) / kTcK;
+  const int nch = (K + kTcK - 1) / kTcK;
   bool ok = true;
   int issued = 0;                                   // stages whose MMAs were committed
   if (err[1]) ok = __syncthreads_and(mbar_wait(mbar_probe, 0, kProbeLimit)) != 0;   // test request: expires
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_update_tc(DevFronts F, const 
         const bool need = op == 0 || !diag;
 #pragma unroll
         for (int e = 0; e < 4; ++e)
-          x[op][u][e] = (need && grow < nf && kk + e < w) ? P[grow + (size_t)(c0 + kk + e) * nf] : 0.0f;
+          x[op][u][e] = (need && grow < nf && kk + e < K) ? P[grow + (size_t)(kbeg + kk + e) * nf] : 0.0f;
       }
 #pragma unroll
     for (int op = 0; op < 2; ++op) {
@@ -278,12 +281,13 @@ cudaError_t prepare_update_tc() {
   return cudaFuncSetAttribute(k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
 }
 
-void launch_update_tc(const DevFronts& F, const int32_t* list, int count, int step, int tiles128, float* panel,
-                      float* upool, int split, int32_t* err, cudaStream_t st, int mode, bool pdl) {
-  const int g = update_grid(tiles128, kTcTile, mode);
-  if (count <= 0 || g <= 0) return;
+int launch_update_tc(const DevFronts& F, const int32_t* list, int count, int step, int T128, float* panel,
+                     float* upool, int split, int32_t* err, cudaStream_t st, UpdBand band, int defer, bool pdl) {
+  const int g = update_grid(T128, kTcTile, band);
+  if (count <= 0 || g <= 0) return 0;
   launch_k(k_update_tc, dim3(g, count), dim3(kTcThreads), kTcSmem, st, pdl, F, list, step, panel, upool, split, err,
-           mode);
+           band.blo, band.bhi, defer);
+  return 1;
 }
 
 }  // namespace mfd

@@ -194,6 +194,30 @@ def test_lookahead_bitwise_equal(precision):
     assert np.array_equal(x0, x1)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_deferred_updates_bitwise_equal(precision):
+    """Deferred trailing updates (reserved[5] = D: the bulk of the trailing
+    matrix takes D panel steps' updates in one pass, the next panel catches up
+    every step) apply every panel step to every entry once and in step order:
+    D = 1..4, with the lookahead schedule and with the serial one, give
+    bit-identical solutions (fronts of 2, 4 and 9 panel steps, partial last
+    panels), which match the oracle."""
+    p = P.laplace3d(32)
+    outs = []
+    for d in (1, 2, 3, 4):
+        for la in (0, 1):
+            s = gpu_for(p, max_zero=1000, precision=precision, reserved=(0, la, 0, 0, 0, d, 0))
+            x = p.rhs.copy()
+            rep, rc = s.solve(x)
+            assert rc == 0
+            outs.append(x)
+            s.close()
+    for x in outs[1:]:
+        assert np.array_equal(outs[0], x)
+    xo = oracle_for(p, max_zero=1000).solve(p.rhs)
+    assert np.abs(outs[0] - xo).max() <= (FP64_X_TOL if precision == 0 else 1e-8) * np.abs(xo).max()
+
+
 def test_programmatic_launch_matches():
     """Programmatic dependent launch along the panel chain (opt-in) gives the
     same factor as the default schedule."""

@@ -95,6 +95,8 @@ typedef struct {
   double time_info[7];      /* the reference's 7 phase timers (time_list_m.f90:3-10), seconds:
                                ordering, analyze, factorize, solve, forward, backward,
                                real_factorize                                                  */
+  int64_t pivot_fallbacks;  /* FP32 factorization: 32-column diagonal sub-blocks whose FP32 pivot
+                               chain met a small pivot and was redone in FP64 (last factorize) */
 } mfd_stats;
 
 /* ---- handle API ------------------------------------------------------------ */

@@ -204,6 +204,7 @@ struct mfd_handle {
 
   bool factored = false;
   bool expire_waits = false;                        // test request (mfd_test_expire_waits)
+  int64_t pivot_fallbacks = 0;                      // FP32 diagonal sub-blocks redone in FP64, last factorize
   int64_t launches_factor = 0, launches_solve = 0;
   double factor_ms = 0, solve_ms = 0, anorm = 0;
   double time_info[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -495,9 +496,10 @@ int upload_plan(mfd_handle* h) {
   CK(h->d_a_src.alloc(h->nnz_total));
   CK(h->d_a_pos.alloc(h->nnz_total));
   CK(h->d_sidx.alloc(h->nnz_total));
-  // [0] first bad pivot column, [1] bounded-wait expiry flag, [2] test request: make the waits expire
-  CK(h->d_info.alloc(3));
-  CK(cudaMemsetAsync(h->d_info.p, 0, 3 * sizeof(int32_t), h->st));
+  // [0] first bad pivot column, [1] bounded-wait expiry flag, [2] test request: make the waits expire,
+  // [3] FP32 diagonal sub-blocks redone in FP64 (small pivot)
+  CK(h->d_info.alloc(4));
+  CK(cudaMemsetAsync(h->d_info.p, 0, 4 * sizeof(int32_t), h->st));
   CK(h->d_cnt.alloc(std::max(1, h->max_large_count)));   // backward-solve tickets, one per list slot
   CK(cudaMemsetAsync(h->d_cnt.p, 0, sizeof(int32_t) * std::max(1, h->max_large_count), h->st));
   DevFronts& F = h->F;
@@ -764,7 +766,8 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
   const int32_t* hl = h->h_lists.data();
   launch_fill_int(h->d_info.p, INT_MAX, 1, st);
   launch_fill_int(h->d_info.p + 1, 0, 1, st);
-  n += 2;
+  launch_fill_int(h->d_info.p + 3, 0, 1, st);
+  n += 3;
   // trailing update: 0 tensor cores (FP64: DMMA; FP32: tcgen05 3xTF32), 1 FFMA tiles, 2 tcgen05 1xTF32 (FP32)
   const int kind = h->opt.reserved[0];
   const bool side = side_streams(h);
@@ -864,7 +867,8 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
         }
       };
       record(h, st, MFD_K_PANEL, pf, pb,
-             [&] { launch_potrf<T>(F, lists + p.off, p.count, (int)s, panel, diag, h->d_info.p, st, pdl); });
+             [&] { launch_potrf<T>(F, lists + p.off, p.count, (int)s, panel, diag, h->d_info.p, st, pdl, 0,
+                                   h->d_info.p + 3); });
       record(h, st, MFD_K_TRSM, tf, tb, [&] {
         launch_trsm<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, kind == 1 ? 1 : 0, st, pdl);
       });
@@ -1050,9 +1054,9 @@ int do_factorize(mfd_handle* h, const double* a) {
                    : run_graph(h, &h->g_factor, [&](cudaStream_t s) { h->launches_factor = enqueue_factor<double>(h, s); });
   if (rc) return rc;
   CK(cudaEventRecord(h->ev1, h->st));
-  int32_t infos[2] = {0, 0};
+  int32_t infos[4] = {0, 0, 0, 0};
   double anorm = 0;
-  CK(cudaMemcpyAsync(infos, h->d_info.p, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaMemcpyAsync(infos, h->d_info.p, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, h->st));
   CK(cudaMemcpyAsync(&anorm, h->d_norms.p + 7, sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   float ms = 0;
@@ -1060,6 +1064,7 @@ int do_factorize(mfd_handle* h, const double* a) {
   collect_profile(h);
   h->factor_ms = ms;
   h->anorm = anorm;
+  h->pivot_fallbacks = infos[3];
   h->time_info[6] = ms * 1e-3;
   h->factored = true;
   const int32_t info = infos[0];
@@ -1460,6 +1465,7 @@ int mfd_get_stats(mfd_handle* h, mfd_stats* st) {
   st->max_front = h->max_nf;
   st->factor_ms = h->factor_ms;
   st->solve_ms = h->solve_ms;
+  st->pivot_fallbacks = h->pivot_fallbacks;
   std::memcpy(st->time_info, h->time_info, sizeof(st->time_info));
   return MFD_OK;
 }

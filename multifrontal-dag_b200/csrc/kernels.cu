@@ -527,10 +527,13 @@ __global__ void __launch_bounds__(256) k_extend_add(DevFronts F, const int32_t* 
 //   k_trsm  : the rows below, X <- A L11^{-T} = A (L11^{-1})^T, a GEMM with K = w
 //   k_update: trailing C(lower) -= P P^T with P the solved panel rows
 
-// Diagonal-block POTRF + inverse, one CTA (8 warps) per front, w <= 128, all
-// arithmetic in FP64 whatever the storage type (the FP32 path's diagonal
-// blocks are thus factored with the FP64 fallback always taken; the kernel is
-// latency bound, so FP64 costs nothing here).
+// Diagonal-block POTRF + inverse, one CTA (8 warps) per front, w <= 128.  The
+// block lives in shared memory in FP64 whatever the storage type.  FP64
+// factorization: every step in FP64.  FP32 factorization: the serial pivot
+// chain of each 32 x 32 diagonal sub-block (and its inverse) runs in FP32,
+// with a fallback to the FP64 chain when a pivot is small (warp_chol32_f32;
+// the `fallbacks` counter counts them); the sub-panel TRSM, the trailing SYRK
+// and the block inverse stay on FP64 DMMA.
 //
 // The block (zero-padded to wp = 32 * ceil(w / 32), identity on the padded
 // diagonal) sits in shared memory S, column-major, ld kPLd.  Right-looking
@@ -660,6 +663,71 @@ __device__ int warp_chol32(double* S, int o, double* D, double* rq, double* cbuf
   return bad;
 }
 
+// The FP64 chain as the FP32 path's fallback, out of line so that its
+// registers do not add to the FP32 chain's.
+__device__ __noinline__ int warp_chol32_fallback(double* S, int o, double* D, double* rq, double* cbuf, int lane) {
+  return warp_chol32(S, o, D, rq, cbuf, lane);
+}
+
+// FP32 form of warp_chol32 for the FP32 factorization: the pivot chain runs
+// in FP32 (rsqrtf, FP32 FMAs) on the block's values as stored, and the
+// factor and its inverse go back to S and D widened to FP64.  A pivot is
+// "small" when it is not positive or below kSmallPivot times the diagonal
+// entry it started from (more than 12 of FP32's 24 significand bits
+// cancelled): the function then returns -1 before writing anything, and the
+// caller redoes the sub-block with the FP64 warp_chol32 (the fallback).  The
+// test is uniform across the warp (the pivot comes from a shuffle, the
+// diagonal entry from shared memory).
+constexpr float kSmallPivot = 1.0f / 4096.0f;
+__device__ int warp_chol32_f32(double* S, int o, double* D, double* rq, float* cbuf, int lane) {
+  float a[kPSub];
+#pragma unroll
+  for (int j = 0; j < kPSub; ++j) a[j] = (float)S[(o + lane) + (o + j) * kPLd];
+  float d = __shfl_sync(0xffffffffu, a[0], 0);
+  if (!(d > kSmallPivot * (float)S[o + o * kPLd])) return -1;
+  float y = rsqrtf(d);
+  float l = a[0] * y;
+#pragma unroll
+  for (int k = 0; k < kPSub; ++k) {
+    float* cb = cbuf + (k & 1) * kPSub;
+    cb[lane] = l;
+    if (lane == 0) rq[o + k] = (double)y;              // the FP64 fallback rewrites rq if it runs
+    a[k] = lane == k ? d * y : l;
+    float dn = 1.0f, yn = 1.0f, ln = 0.0f;
+    if (k + 1 < kPSub) {
+      a[k + 1] = fmaf(-l, __shfl_sync(0xffffffffu, l, k + 1), a[k + 1]);
+      dn = __shfl_sync(0xffffffffu, a[k + 1], k + 1);
+      const float dk = (float)S[(o + k + 1) * (kPLd + 1)];
+      if (!(dn > kSmallPivot * dk)) return -1;          // uniform: small pivot, FP64 fallback
+      yn = rsqrtf(dn);
+      ln = a[k + 1] * yn;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = k + 2; j < kPSub; ++j) a[j] = fmaf(-l, cb[j], a[j]);
+    d = dn;
+    y = yn;
+    l = ln;
+  }
+#pragma unroll
+  for (int j = 0; j < kPSub; ++j)
+    if (j <= lane) S[(o + lane) + (o + j) * kPLd] = (double)a[j];
+  __syncwarp();
+  // inverse: lane j owns column j of X = L^{-1}; forward substitution on e_j (FP32)
+  float x[kPSub];
+#pragma unroll
+  for (int i = 0; i < kPSub; ++i) x[i] = i == lane ? 1.0f : 0.0f;
+#pragma unroll
+  for (int k = 0; k < kPSub; ++k) {
+    x[k] *= (float)rq[o + k];
+#pragma unroll
+    for (int i = k + 1; i < kPSub; ++i) x[i] = fmaf(-(float)S[(o + i) + (o + k) * kPLd], x[k], x[i]);
+  }
+#pragma unroll
+  for (int i = 0; i < kPSub; ++i) D[i + lane * kDLd] = (double)x[i];
+  return 0;
+}
+
 // Inverted diagonal block of panel step `step` of front f: persistent per front
 // when the plan provides d_off (kept for the solves), else one slot per list
 // entry of the launch.
@@ -668,10 +736,12 @@ __device__ __forceinline__ T* inv_block(const DevFronts& F, T* linv, int f, int 
   return F.d_off ? linv + F.d_off[f] + (size_t)step * kFactB * kFactB : linv + (size_t)slot * kFactB * kFactB;
 }
 
-// info_stride 0: every front reports into info[0]; 1: list slot i reports into info[i]
+// info_stride 0: every front reports into info[0]; 1: list slot i reports into info[i].
+// fallbacks (may be null): counts the FP32 sub-blocks redone in FP64.
 template <typename T>
 __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const int32_t* list, int step, T* panel,
-                                                            T* linv, int32_t* info, int info_stride) {
+                                                            T* linv, int32_t* info, int info_stride,
+                                                            int32_t* fallbacks) {
   constexpr int B = kFactB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* S = reinterpret_cast<double*>(smem_raw);
@@ -727,7 +797,16 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
     const int o = b * kPSub;
     double* Db = Dv + (size_t)b * kPSub * kDLd;
     if (warp == 0) {
-      const int bad = warp_chol32(S, o, Db, rq, cbuf, lane);
+      int bad;
+      if constexpr (sizeof(T) == 4) {
+        bad = warp_chol32_f32(S, o, Db, rq, reinterpret_cast<float*>(cbuf), lane);
+        if (bad < 0) {                                   // small pivot: the FP64 chain
+          if (lane == 0 && fallbacks) atomicAdd(fallbacks, 1);
+          bad = warp_chol32_fallback(S, o, Db, rq, cbuf, lane);
+        }
+      } else {
+        bad = warp_chol32(S, o, Db, rq, cbuf, lane);
+      }
       if (bad && lane == 0 && o + bad <= w) atomicMin(info + (size_t)info_stride * blockIdx.x, F.first[f] + c0 + o + bad);
     }
     __syncthreads();
@@ -2357,10 +2436,10 @@ void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int m
 }
 template <typename T>
 void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
-                  cudaStream_t st, bool pdl, int info_stride) {
+                  cudaStream_t st, bool pdl, int info_stride, int32_t* fallbacks) {
   if (count <= 0) return;
   launch_k(k_potrf<T>, dim3(count), dim3(kPotrfThreads), kPotrfSmem, st, pdl, F, list, step, panel, linv, info,
-           info_stride);
+           info_stride, fallbacks);
 }
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
@@ -2525,7 +2604,7 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
                                          cudaStream_t);                                                            \
   template void launch_extend_add<T>(const DevFronts&, const int32_t*, int, int, T*, T*, cudaStream_t);             \
   template void launch_potrf<T>(const DevFronts&, const int32_t*, int, int, T*, T*, int32_t*, cudaStream_t, bool,  \
-                                int);                                                                              \
+                                int, int32_t*);                                                                    \
   template void launch_trsm<T>(const DevFronts&, const int32_t*, int, int, int, T*, const T*, int, cudaStream_t,   \
                                bool);                                                                              \
   template int launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t,    \

@@ -135,10 +135,12 @@ void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int m
 //            one 128 x 128 slot per list entry when d_off is null)
 //   trsm   : rows below the diagonal block, X <- X L11^{-T}   (kind 0: DMMA, 1: FMA)
 //   update : trailing lower triangle -= P P^T                  (kind 0: DMMA 128-tiles, 1: FMA 64-tiles)
-// info_stride 0: the first bad pivot of any front goes to info[0] (atomic min); 1: list slot i's to info[i]
+// info_stride 0: the first bad pivot of any front goes to info[0] (atomic min); 1: list slot i's to info[i].
+// FP32: the diagonal sub-blocks' pivot chains run in FP32 with an FP64 fallback on a small pivot;
+// fallbacks (may be null) counts the sub-blocks redone in FP64.
 template <typename T>
 void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
-                  cudaStream_t st, bool pdl = false, int info_stride = 0);
+                  cudaStream_t st, bool pdl = false, int info_stride = 0, int32_t* fallbacks = nullptr);
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
                  const T* linv, int kind, cudaStream_t st, bool pdl = false);

@@ -60,7 +60,7 @@ class Stats(C.Structure):
                 ("cost", C.c_int64), ("nonzero", C.c_int64), ("panel_bytes", C.c_int64),
                 ("update_pool_bytes", C.c_int64), ("launches_factor", C.c_int64), ("launches_solve", C.c_int64),
                 ("max_front", C.c_int64), ("factor_ms", C.c_double), ("solve_ms", C.c_double),
-                ("time_info", C.c_double * 7)]
+                ("time_info", C.c_double * 7), ("pivot_fallbacks", C.c_int64)]
 
 
 EXPORTS = [

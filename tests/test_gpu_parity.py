@@ -390,6 +390,49 @@ def test_fp32_tensor_update_against_ffma(variant, tol):
     assert rc == 0 and rep.backward_error <= 1e-12
 
 
+def _dense_lower_ccs(a):
+    n = a.shape[0]
+    ptr, rows, vals = [1], [], []
+    for j in range(n):
+        rows.extend(range(j + 1, n + 1))
+        vals.extend(a[j:, j])
+        ptr.append(len(rows) + 1)
+    return np.array(ptr, np.int32), np.array(rows, np.int32), np.array(vals, np.float64)
+
+
+@pytest.mark.parametrize("small", [1e-4, None], ids=["small_pivot", "well_conditioned"])
+def test_fp32_potrf_small_pivot_falls_back_to_fp64(small):
+    """The FP32 factorization's diagonal blocks run their pivot chain in FP32
+    and redo a 32-column sub-block in FP64 when a pivot falls below 2^-12 of
+    the diagonal entry it started from.  A dense SPD front A = L diag(d) L^T
+    (n = 300: one front, three 128-column panel steps on the blocked path)
+    whose pivot 41 is d_41 = 1e-4 x its column's scale triggers the fallback;
+    refinement reaches 1e-12 and x matches the FP64 solution.  Without the
+    small pivot no sub-block falls back."""
+    n = 300
+    rng = np.random.default_rng(8)
+    L = np.tril(rng.uniform(-0.3, 0.3, (n, n)), -1) + np.eye(n)
+    d = rng.uniform(1.0, 2.0, n)
+    if small is not None:
+        d[40] = small
+    A = (L * d) @ L.T
+    col, row, val = _dense_lower_ccs(A)
+    s = H.Solver.analyze(n, col, row, None, max_zero=0, precision=H.MFD_PREC_FP32_IR)
+    assert s.stats().num_front == 1 and s.stats().max_front == n
+    assert s.factorize(val) == 0
+    fb = s.stats().pivot_fallbacks
+    assert (fb >= 1) if small is not None else (fb == 0), fb
+    xt = rng.uniform(-1, 1, n)
+    b = A @ xt
+    x = b.copy()
+    rep, rc = s.solve(x)
+    assert rc == 0 and rep.converged == 1 and rep.backward_error <= 1e-12
+    xr = np.linalg.solve(A, b)
+    assert np.abs(x - xr).max() <= 1e-8 * np.abs(xr).max()
+    s64 = H.Solver.analyze(n, col, row, None, max_zero=0)
+    assert s64.factorize(val) == 0 and s64.stats().pivot_fallbacks == 0
+
+
 @pytest.mark.parametrize("k", [10, 37])
 def test_fp32_ir_many_rhs(k):
     """Block refinement: all right-hand sides refined together (residuals of

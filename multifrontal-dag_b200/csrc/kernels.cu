@@ -670,21 +670,25 @@ __device__ __noinline__ int warp_chol32_fallback(double* S, int o, double* D, do
 }
 
 // FP32 form of warp_chol32 for the FP32 factorization: the pivot chain runs
-// in FP32 (rsqrtf, FP32 FMAs) on the block's values as stored, and the
-// factor and its inverse go back to S and D widened to FP64.  A pivot is
+// in FP32 (rsqrtf, FP32 FMAs) on the block's values as stored; the factor
+// goes back to S widened to FP64 and, as FP32, to Fb (32 x 33 floats), from
+// which the inverse is formed in FP32 and written to D in FP64.  A pivot is
 // "small" when it is not positive or below kSmallPivot times the diagonal
 // entry it started from (more than 12 of FP32's 24 significand bits
-// cancelled): the function then returns -1 before writing anything, and the
+// cancelled): the function then returns -1 before writing S or D, and the
 // caller redoes the sub-block with the FP64 warp_chol32 (the fallback).  The
 // test is uniform across the warp (the pivot comes from a shuffle, the
 // diagonal entry from shared memory).
 constexpr float kSmallPivot = 1.0f / 4096.0f;
-__device__ int warp_chol32_f32(double* S, int o, double* D, double* rq, float* cbuf, int lane) {
-  float a[kPSub];
+constexpr int kFbLd = kPSub + 1;
+__device__ int warp_chol32_f32(double* S, int o, double* D, double* rq, float* cbuf, float* Fb, int lane) {
+  float a[kPSub], dg[kPSub];
 #pragma unroll
   for (int j = 0; j < kPSub; ++j) a[j] = (float)S[(o + lane) + (o + j) * kPLd];
+#pragma unroll
+  for (int j = 0; j < kPSub; ++j) dg[j] = __shfl_sync(0xffffffffu, a[j], j) * kSmallPivot;   // small-pivot bounds
   float d = __shfl_sync(0xffffffffu, a[0], 0);
-  if (!(d > kSmallPivot * (float)S[o + o * kPLd])) return -1;
+  if (!(d > dg[0])) return -1;
   float y = rsqrtf(d);
   float l = a[0] * y;
 #pragma unroll
@@ -697,8 +701,7 @@ __device__ int warp_chol32_f32(double* S, int o, double* D, double* rq, float* c
     if (k + 1 < kPSub) {
       a[k + 1] = fmaf(-l, __shfl_sync(0xffffffffu, l, k + 1), a[k + 1]);
       dn = __shfl_sync(0xffffffffu, a[k + 1], k + 1);
-      const float dk = (float)S[(o + k + 1) * (kPLd + 1)];
-      if (!(dn > kSmallPivot * dk)) return -1;          // uniform: small pivot, FP64 fallback
+      if (!(dn > dg[k + 1])) return -1;                  // uniform: small pivot, FP64 fallback
       yn = rsqrtf(dn);
       ln = a[k + 1] * yn;
     }
@@ -710,8 +713,10 @@ __device__ int warp_chol32_f32(double* S, int o, double* D, double* rq, float* c
     l = ln;
   }
 #pragma unroll
-  for (int j = 0; j < kPSub; ++j)
+  for (int j = 0; j < kPSub; ++j) {
+    Fb[lane + j * kFbLd] = a[j];
     if (j <= lane) S[(o + lane) + (o + j) * kPLd] = (double)a[j];
+  }
   __syncwarp();
   // inverse: lane j owns column j of X = L^{-1}; forward substitution on e_j (FP32)
   float x[kPSub];
@@ -721,7 +726,7 @@ __device__ int warp_chol32_f32(double* S, int o, double* D, double* rq, float* c
   for (int k = 0; k < kPSub; ++k) {
     x[k] *= (float)rq[o + k];
 #pragma unroll
-    for (int i = k + 1; i < kPSub; ++i) x[i] = fmaf(-(float)S[(o + i) + (o + k) * kPLd], x[k], x[i]);
+    for (int i = k + 1; i < kPSub; ++i) x[i] = fmaf(-Fb[i + k * kFbLd], x[k], x[i]);
   }
 #pragma unroll
   for (int i = 0; i < kPSub; ++i) D[i + lane * kDLd] = (double)x[i];
@@ -799,7 +804,8 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
     if (warp == 0) {
       int bad;
       if constexpr (sizeof(T) == 4) {
-        bad = warp_chol32_f32(S, o, Db, rq, reinterpret_cast<float*>(cbuf), lane);
+        // Yv (the inverse phase's scratch) is free here: the sub-block's FP32 copy
+        bad = warp_chol32_f32(S, o, Db, rq, reinterpret_cast<float*>(cbuf), reinterpret_cast<float*>(Yv), lane);
         if (bad < 0) {                                   // small pivot: the FP64 chain
           if (lane == 0 && fallbacks) atomicAdd(fallbacks, 1);
           bad = warp_chol32_fallback(S, o, Db, rq, cbuf, lane);

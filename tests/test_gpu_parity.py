@@ -198,24 +198,32 @@ def test_lookahead_bitwise_equal(precision):
 def test_deferred_updates_bitwise_equal(precision):
     """Deferred trailing updates (reserved[5] = D: the bulk of the trailing
     matrix takes D panel steps' updates in one pass, the next panel catches up
-    every step) apply every panel step to every entry once and in step order:
-    D = 1..4, with the lookahead schedule and with the serial one, give
-    bit-identical solutions (fronts of 2, 4 and 9 panel steps, partial last
-    panels), which match the oracle."""
+    every step) apply every panel step to every entry once and in step order.
+    For each D the lookahead schedule and the serial one give bit-identical
+    solutions (fronts of 2, 4 and 9 panel steps, partial last panels).  In
+    FP64 the accumulators start from C, so D = 1..4 are bit-identical too; the
+    FP32 tensor-core update accumulates each pass from zero in TMEM and
+    subtracts at the end, so there D changes the rounding and the refined
+    solutions agree to the refinement tolerance.  All match the oracle."""
     p = P.laplace3d(32)
-    outs = []
+    outs = {}
     for d in (1, 2, 3, 4):
         for la in (0, 1):
             s = gpu_for(p, max_zero=1000, precision=precision, reserved=(0, la, 0, 0, 0, d, 0))
             x = p.rhs.copy()
             rep, rc = s.solve(x)
             assert rc == 0
-            outs.append(x)
+            outs[d, la] = x
             s.close()
-    for x in outs[1:]:
-        assert np.array_equal(outs[0], x)
+        assert np.array_equal(outs[d, 0], outs[d, 1]), d
+    x1 = outs[1, 0]
+    for d in (2, 3, 4):
+        if precision == 0:
+            assert np.array_equal(x1, outs[d, 0]), d
+        else:
+            assert np.abs(outs[d, 0] - x1).max() <= 1e-9 * np.abs(x1).max(), d
     xo = oracle_for(p, max_zero=1000).solve(p.rhs)
-    assert np.abs(outs[0] - xo).max() <= (FP64_X_TOL if precision == 0 else 1e-8) * np.abs(xo).max()
+    assert np.abs(x1 - xo).max() <= (FP64_X_TOL if precision == 0 else 1e-8) * np.abs(xo).max()
 
 
 def test_programmatic_launch_matches():
@@ -400,15 +408,17 @@ def _dense_lower_ccs(a):
     return np.array(ptr, np.int32), np.array(rows, np.int32), np.array(vals, np.float64)
 
 
-@pytest.mark.parametrize("small", [1e-4, None], ids=["small_pivot", "well_conditioned"])
+@pytest.mark.parametrize("small", [1e-4, None], ids=["small_pivot", "no_small_pivot"])
 def test_fp32_potrf_small_pivot_falls_back_to_fp64(small):
     """The FP32 factorization's diagonal blocks run their pivot chain in FP32
     and redo a 32-column sub-block in FP64 when a pivot falls below 2^-12 of
     the diagonal entry it started from.  A dense SPD front A = L diag(d) L^T
     (n = 300: one front, three 128-column panel steps on the blocked path)
     whose pivot 41 is d_41 = 1e-4 x its column's scale triggers the fallback;
-    refinement reaches 1e-12 and x matches the FP64 solution.  Without the
-    small pivot no sub-block falls back."""
+    refinement reaches 1e-12, and x matches the FP64 solution within
+    10 cond(A) times the refinement tolerance (the forward error a solution
+    with backward error 1e-12 can have).  Without the small pivot no
+    sub-block falls back."""
     n = 300
     rng = np.random.default_rng(8)
     L = np.tril(rng.uniform(-0.3, 0.3, (n, n)), -1) + np.eye(n)
@@ -428,7 +438,7 @@ def test_fp32_potrf_small_pivot_falls_back_to_fp64(small):
     rep, rc = s.solve(x)
     assert rc == 0 and rep.converged == 1 and rep.backward_error <= 1e-12
     xr = np.linalg.solve(A, b)
-    assert np.abs(x - xr).max() <= 1e-8 * np.abs(xr).max()
+    assert np.abs(x - xr).max() <= 10 * np.linalg.cond(A) * 1e-12 * np.abs(xr).max()
     s64 = H.Solver.analyze(n, col, row, None, max_zero=0)
     assert s64.factorize(val) == 0 and s64.stats().pivot_fallbacks == 0
 

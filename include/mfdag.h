@@ -54,9 +54,11 @@ typedef struct {
   int32_t small_front_max; /* fronts up to this order run in the fused one-CTA kernel (0=auto)*/
   int32_t panel_width;     /* column panel of the blocked large-front factorization (0=auto) */
   int32_t reserved[7];     /* schedule switches, 0 = default: [0] trailing-update kind (1 FFMA
-                              tiles, 2 single-pass TF32), [1] = 1 lookahead off, [2] = 1
-                              programmatic launch along the panel chain, [3] = 1 no programmatic
-                              launch between solve steps, [4] = 1 no side streams per level     */
+                              tiles, 2 single-pass TF32, 3 FP64 DMMA in whole 128 x 128 tiles),
+                              [1] = 1 lookahead off, [2] = 1 programmatic launch along the panel
+                              chain, [3] = 1 no programmatic launch between solve steps, [4] = 1
+                              no side streams per level, [5] = panel steps per deferred trailing
+                              update (1 = none)                                                 */
 } mfd_options;
 
 /* Symbolic data exactly as the reference holds it after hppllt_analyze

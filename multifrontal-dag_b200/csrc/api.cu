@@ -768,7 +768,8 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
   launch_fill_int(h->d_info.p + 1, 0, 1, st);
   launch_fill_int(h->d_info.p + 3, 0, 1, st);
   n += 3;
-  // trailing update: 0 tensor cores (FP64: DMMA; FP32: tcgen05 3xTF32), 1 FFMA tiles, 2 tcgen05 1xTF32 (FP32)
+  // trailing update: 0 tensor cores (FP64: DMMA in 128 x 64 halves, two CTAs per SM; FP32: tcgen05 3xTF32),
+  // 1 FFMA tiles, 2 tcgen05 1xTF32 (FP32), 3 FP64 DMMA in whole 128 x 128 tiles, one CTA per SM
   const int kind = h->opt.reserved[0];
   const bool side = side_streams(h);
   for (const LevelPlan& L : h->levels) {
@@ -887,7 +888,7 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
             }
           }
           n += launch_update<T>(F, lists + p.off, p.count, (int)s, p.param2, p.param3, panel, upool,
-                                kind == 1 ? 1 : 0, us, band, D, upd_pdl && kind != 1);
+                                kind == 1 || kind == 3 ? kind : 0, us, band, D, upd_pdl && kind != 1);
         });
       };
       if (!lookahead || s + 1 == L.steps.size()) {

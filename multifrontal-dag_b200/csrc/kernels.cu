@@ -1111,6 +1111,142 @@ __global__ void __launch_bounds__(kUThreads, 1) k_update_dmma(DevFronts F, const
       }
 }
 
+// FP64 trailing update in 128 x 64 halves: CTA x computes columns
+// 64 h .. 64 h + 63 (h = x & 1) of square tile x >> 1 of the band (the same
+// tiles, bands and K ranges as k_update_dmma).  256 threads: 8 warps as 4
+// (rows) x 2 (columns) of 32 x 32, each 2 x 4 mma.m16n8k16.f64 per K step of
+// 16, so 128 registers and 102 KB of shared memory per CTA and two CTAs per
+// SM: one CTA's C loads and stores overlap the other's MMAs.  Operands come
+// in K chunks of 32 by cp.async, double-buffered; a diagonal tile's B is rows
+// 64 h .. of its A.  C is loaded into the accumulators (the A fragments enter
+// negated) and stored back; tiles wholly inside the trailing matrix, below
+// the diagonal and inside the panel or the update matrix take an unchecked
+// path.  In a diagonal tile's right half the warps whose 32 rows all lie
+// above the diagonal skip the MMAs.
+constexpr int kU2Threads = 256;
+constexpr int kU2N = 64;
+constexpr int kU2LdB = kU2N + 4;                             // 68 = 4 mod 16 doubles: conflict-free fragments
+constexpr int kU2Stage = kUK * kULD + kUK * kU2LdB;           // doubles per pipeline stage
+constexpr size_t kU2Smem = 2 * (size_t)kU2Stage * sizeof(double);
+
+__global__ void __launch_bounds__(kU2Threads, 2) k_update_dmma2(DevFronts F, const int32_t* list, int step,
+                                                              double* panel, double* upool, int blo, int bhi,
+                                                              int defer) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* sm = reinterpret_cast<double*>(smem_raw);     // per stage: A [k][kULD] (128 rows), B [k][kU2LdB] (64 rows)
+  const int f = list[blockIdx.y];
+  const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
+  const int c0 = step * kFactB;
+  if (c0 >= nc) return;
+  const int w = min(kFactB, nc - c0);
+  const int base = c0 + w;
+  const int nrem = nf - base;
+  if (nrem <= 0) return;
+  const int T = (nrem + kUT - 1) / kUT;
+  const int hf = blockIdx.x & 1;
+  int ti, tj, kbeg, kend;
+  if (!select_tile(T, kUT, blo, bhi, blockIdx.x >> 1, ti, tj)) return;
+  if (!update_k_range(nc, step, defer, tj, kUT, kbeg, kend)) return;
+  const int i0 = base + ti * kUT, j0 = base + tj * kUT + hf * kU2N;
+  if (j0 >= nf) return;                                 // the right half lies beyond the matrix
+  const int K = kend - kbeg;                            // panel columns [kbeg, kend) of the front
+  const bool diag = ti == tj;
+  double* P = panel + F.panel_off[f];
+  double* U = upool + F.u_off[f];
+  const int nchunks = (K + kUK - 1) / kUK;
+  auto load = [&](int stage, int kc) {
+    double* dst = sm + stage * kU2Stage;
+    const int ne = diag ? kUK * kUT : kUK * (kUT + kU2N);    // a diagonal tile's B is in A
+    for (int e = threadIdx.x; e < ne; e += kU2Threads) {
+      int k, row;
+      double* d;
+      if (e < kUK * kUT) {
+        k = e >> 7; const int r = e & (kUT - 1);
+        row = i0 + r; d = dst + k * kULD + r;
+      } else {
+        const int e2 = e - kUK * kUT;
+        k = e2 >> 6; const int r = e2 & (kU2N - 1);
+        row = j0 + r; d = dst + kUK * kULD + k * kU2LdB + r;
+      }
+      const int col = kc * kUK + k;
+      const bool valid = row < nf && col < K;
+      cp_async8(d, valid ? P + row + (size_t)(kbeg + col) * nf : P, valid);
+    }
+    cp_async_commit();
+  };
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int g = lane >> 2, q = lane & 3;
+  const int rbase = i0 + wm * 32 + g, cbase = j0 + wn * 32 + 2 * q;
+  // warps of a diagonal tile's right half whose rows all lie above the diagonal
+  const bool idle = i0 + wm * 32 + 31 < j0 + wn * 32;
+  // unchecked path: the tile is inside the trailing matrix, wholly below the
+  // diagonal and wholly in the panel or wholly in the update matrix
+  const bool full = i0 + kUT <= nf && j0 + kU2N <= nf && i0 >= j0 + kU2N && (j0 + kU2N <= nc || j0 >= nc);
+  const int ldc = j0 < nc ? nf : nr;
+  double* Cb = j0 < nc ? P + (size_t)j0 * nf : U + (size_t)(j0 - nc) * nr - nc;   // C(gi, gj) = Cb[gi + (gj - j0) ldc]
+  pdl_wait();
+  pdl_trigger();
+  load(0, 0);
+  double acc[2][4][4];
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int gi = rbase + mi * 16 + 8 * (e >> 1), gj = cbase + ni * 8 + (e & 1);
+        if (full)
+          acc[mi][ni][e] = Cb[gi + (size_t)(gj - j0) * ldc];
+        else
+          acc[mi][ni][e] = (!idle && gi < nf && gj < nf && gi >= gj) ? *trailing_addr(P, U, nc, nr, nf, gi, gj) : 0.0;
+      }
+  for (int kc = 0; kc < nchunks; ++kc) {
+    if (kc + 1 < nchunks) {
+      load((kc + 1) & 1, kc + 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    if (!idle) {
+      const double* As = sm + (kc & 1) * kU2Stage;
+      const double* Bs = diag ? As + hf * kU2N : As + kUK * kULD;
+      const int ldb = diag ? kULD : kU2LdB;
+#pragma unroll
+      for (int kk = 0; kk < kUK; kk += 16) {
+        double bv[4][4];
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) bv[ni][i] = Bs[(kk + q + 4 * i) * ldb + wn * 32 + ni * 8 + g];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+          double av[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) av[i] = -As[(kk + q + 4 * (i >> 1)) * kULD + wm * 32 + mi * 16 + g + 8 * (i & 1)];
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) dmma16(acc[mi][ni], av, bv[ni]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (idle) return;
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int gi = rbase + mi * 16 + 8 * (e >> 1), gj = cbase + ni * 8 + (e & 1);
+        if (full)
+          Cb[gi + (size_t)(gj - j0) * ldc] = acc[mi][ni][e];
+        else if (gi < nf && gj < nf && gi >= gj)
+          *trailing_addr(P, U, nc, nr, nf, gi, gj) = acc[mi][ni][e];
+      }
+}
+
 // Trailing update on the FMA pipes (any T): 64x64 tiles, K in chunks of 64,
 // 256 threads each 4x4 outputs (rows ty+16m, columns tx+16n).
 constexpr int kSimtTile = 64, kSimtK = 64;
@@ -2380,6 +2516,7 @@ cudaError_t prepare_kernels() {
   chk(opt_in(k_potrf<double>)); chk(opt_in(k_potrf<float>));
   chk(prepare_update_tc());
   chk(opt_in(k_update_simt<double>)); chk(opt_in(k_update_simt<float>));
+  chk(opt_in(k_update_dmma2));
   return e;
 }
 
@@ -2468,7 +2605,14 @@ int launch_update(const DevFronts& F, const int32_t* list, int count, int step, 
                   T* upool, int kind, cudaStream_t st, UpdBand band, int defer, bool pdl) {
   if (count <= 0) return 0;
   if constexpr (sizeof(T) == 8) {
-    if (kind == 0) {
+    if (kind == 0) {                                   // 128 x 64 halves, two CTAs per SM
+      const int g = update_grid(T128, kUT, band);
+      if (g <= 0) return 0;
+      launch_k(k_update_dmma2, dim3(2 * g, count), dim3(kU2Threads), kU2Smem, st, pdl, F, list, step,
+               reinterpret_cast<double*>(panel), reinterpret_cast<double*>(upool), band.blo, band.bhi, defer);
+      return 1;
+    }
+    if (kind == 3) {                                   // whole 128 x 128 tiles, one CTA per SM
       const int g = update_grid(T128, kUT, band);
       if (g <= 0) return 0;
       size_t sm = 2 * 2 * (size_t)kUK * kULD * sizeof(double);

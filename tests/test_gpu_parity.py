@@ -166,18 +166,41 @@ def test_wide_panels_many_rows(precision):
 
 
 def test_update_kernel_variants_agree():
-    """DMMA and FFMA trailing updates give the same factor to rounding."""
+    """FP64 trailing-update variants: the 128 x 64 half-tile DMMA kernel (the
+    default) and the whole-tile one apply the same DMMA sequence to every
+    entry (bit-identical); the FFMA tiles agree to rounding."""
     p = P.laplace3d(14)
     s0 = gpu_for(p, small_front_max=40)
-    opts = H.default_options(small_front_max=40)
-    s1 = H.Solver.analyze(p.n, p.col, p.row, p.order, max_zero=10, small_front_max=40,
-                          reserved=(1, 0, 0, 0, 0, 0, 0))
-    assert s1.factorize(p.val) == 0
-    x0, x1 = p.rhs.copy(), p.rhs.copy()
+    s1 = gpu_for(p, small_front_max=40, reserved=(1, 0, 0, 0, 0, 0, 0))
+    s3 = gpu_for(p, small_front_max=40, reserved=(3, 0, 0, 0, 0, 0, 0))
+    x0, x1, x3 = p.rhs.copy(), p.rhs.copy(), p.rhs.copy()
     s0.solve(x0)
     s1.solve(x1)
+    s3.solve(x3)
+    assert np.array_equal(x0, x3)
     assert np.abs(x0 - x1).max() <= 1e-12 * np.abs(x0).max()
-    del opts
+
+
+def test_dense_front_update_variants_bitwise():
+    """One dense front (n = 700: six panel steps, tiles on both sides of the
+    panel / update-matrix boundary with a partial last panel, max_zero = 0)
+    factored with both DMMA update kernels: identical factors; the solution
+    matches numpy's."""
+    n = 700
+    rng = np.random.default_rng(12)
+    M = rng.standard_normal((n, n))
+    A = M @ M.T / n + 2.0 * np.eye(n)
+    col, row, val = _dense_lower_ccs(A)
+    out = []
+    for kind in (0, 3):
+        s = H.Solver.analyze(n, col, row, None, max_zero=0, reserved=(kind, 0, 0, 0, 0, 2, 0))
+        assert s.factorize(val) == 0
+        out.append(s.front_panel(1))
+        b = A @ np.ones(n)
+        x = b.copy()
+        rep, rc = s.solve(x)
+        assert rc == 0 and np.abs(x - 1.0).max() <= 1e-10
+    assert np.array_equal(out[0], out[1])
 
 
 @pytest.mark.parametrize("precision", [0, 1])

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -69,29 +70,23 @@ struct DBuf {
 };
 
 // best-fit allocator over a simulated address space (static memory plan):
-// free blocks indexed by address (for coalescing) and by size (for the
-// search), so a plan over millions of fronts stays O(F log F)
+// free blocks indexed by address (for coalescing) and by (size, address) (for
+// the search; erasing one block is O(log F) even when thousands of blocks have
+// the same size, as in a batch of equal systems), so a plan over millions of
+// fronts stays O(F log F)
 struct BestFit {
   std::map<int64_t, int64_t> by_addr;            // offset -> size
-  std::multimap<int64_t, int64_t> by_size;       // size -> offset
+  std::set<std::pair<int64_t, int64_t>> by_size; // (size, offset)
   int64_t top = 0;
-  void erase_size(int64_t size, int64_t off) {
-    auto r = by_size.equal_range(size);
-    for (auto it = r.first; it != r.second; ++it)
-      if (it->second == off) {
-        by_size.erase(it);
-        return;
-      }
-  }
   void insert(int64_t off, int64_t size) {
     by_addr[off] = size;
     by_size.emplace(size, off);
   }
   int64_t alloc(int64_t size) {
     size = align_up(std::max<int64_t>(size, 1));
-    auto it = by_size.lower_bound(size);
+    auto it = by_size.lower_bound({size, INT64_MIN});
     if (it != by_size.end()) {
-      int64_t off = it->second, have = it->first;
+      int64_t have = it->first, off = it->second;
       by_size.erase(it);
       by_addr.erase(off);
       if (have > size) insert(off + size, have - size);
@@ -102,7 +97,7 @@ struct BestFit {
       auto last = std::prev(by_addr.end());
       if (last->first + last->second == top) {
         int64_t off = last->first;
-        erase_size(last->second, off);
+        by_size.erase({last->second, off});
         by_addr.erase(last);
         top = off + size;
         return off;
@@ -117,7 +112,7 @@ struct BestFit {
     auto nx = by_addr.lower_bound(off);
     if (nx != by_addr.end() && off + size == nx->first) {
       size += nx->second;
-      erase_size(nx->second, nx->first);
+      by_size.erase({nx->second, nx->first});
       nx = by_addr.erase(nx);
     }
     if (nx != by_addr.begin()) {
@@ -125,7 +120,7 @@ struct BestFit {
       if (pv->first + pv->second == off) {
         off = pv->first;
         size += pv->second;
-        erase_size(pv->second, pv->first);
+        by_size.erase({pv->second, pv->first});
         by_addr.erase(pv);
       }
     }

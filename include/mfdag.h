@@ -99,6 +99,9 @@ typedef struct {
                                real_factorize                                                  */
   int64_t pivot_fallbacks;  /* FP32 factorization: 32-column diagonal sub-blocks whose FP32 pivot
                                chain met a small pivot and was redone in FP64 (last factorize) */
+  double setup_s[4];        /* handle set-up, seconds: host symbolic analysis (mfd_analyze*),
+                               level / memory plan, device index maps and their exports,
+                               residual CSR and numeric storage                                */
 } mfd_stats;
 
 /* ---- handle API ------------------------------------------------------------ */
@@ -133,6 +136,42 @@ int mfd_symbolic_free(mfd_analysis *a);
 /* Batch analysis: system s is (n[s], ccs_col[s], ccs_row[s], order_perm[s]). */
 int mfd_analyze_batch(mfd_handle **h, int32_t num_systems, const int32_t *n, const int32_t *const *ccs_col,
                       const int32_t *const *ccs_row, const int32_t *const *order_perm, const mfd_options *opt);
+
+/* ---- input formats (the step before hppllt_analyze) ----------------------------
+ * The reference's driver reads a Matrix Market file and converts its COO lists
+ * to CCS before calling hppllt_analyze (example.f90:63-145).
+ *
+ * mfd_mm_read replaces read_data (example.f90:63-93): '%' lines are skipped,
+ * then "n n nnz" and nnz lines "row col value" (1-based; pattern files get
+ * value 1).  The arrays are allocated on the host; free them with mfd_coo_free.
+ *
+ * mfd_coo_to_ccs replaces coo_to_ccs (example.f90:95-145) and runs on GPU
+ * `device`: CCS column pointers (n+1), rows and values (nnz), 1-based, rows
+ * ascending in each column and entries with equal (row, col) in reverse input
+ * order, as the reference's two counting sorts leave them.  Pointers may be
+ * host or device memory (inputs and outputs each all one kind); val and
+ * ccs_val may both be NULL (structure only).  An index outside 1..n is
+ * MFD_E_ARG.
+ *
+ * mfd_analyze_csr: direct CSR input (no counterpart in the reference).  The
+ * CSR (row pointers n+1, column indices; `base` 0 or 1) holds the lower
+ * triangle or the whole symmetric matrix (entries above the diagonal are
+ * ignored; the CSR of the upper triangle is the lower CCS and goes to
+ * mfd_analyze as it is).  Its lower triangle is converted to CCS on the GPU
+ * and analysed as by mfd_analyze; afterwards mfd_factorize takes the values
+ * in the caller's CSR order (csr_ptr[n] - base of them). */
+typedef struct {
+  int32_t n;
+  int64_t nnz;
+  int32_t *row, *col;       /* 1-based coordinates, nnz each */
+  double *val;
+} mfd_coo;
+int mfd_mm_read(const char *path, mfd_coo *out);
+void mfd_coo_free(mfd_coo *coo);
+int mfd_coo_to_ccs(int32_t n, int64_t nnz, const int32_t *row, const int32_t *col, const double *val,
+                   int32_t *ccs_col, int32_t *ccs_row, double *ccs_val, int32_t device);
+int mfd_analyze_csr(mfd_handle **h, int32_t n, const int32_t *csr_ptr, const int32_t *csr_col, int32_t base,
+                    const int32_t *order_perm, const mfd_options *opt);
 
 /* Replaces the body of hppllt_factorize (hppllt.f90:134-149): permutate,
  * set_zero, set_coefficient, seq/StarPU factorize.  a: original-order lower-CCS

@@ -41,7 +41,7 @@ int fail(int code, const std::string& msg) {
 
 constexpr int64_t kAlign = 32;  // elements; keeps every front 256-byte aligned in FP64
 constexpr int kResMulti = 4;     // from this many right-hand sides on, one multi-column residual per IR sweep
-constexpr int kDeferDefault = 2; // panel steps per deferred trailing update (K up to 2 x 128)
+constexpr int kDeferDefault = 1; // panel steps per deferred trailing update (measured: deferring costs time)
 int64_t align_up(int64_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 template <typename T>
@@ -135,6 +135,10 @@ struct SmallBin {
 }  // namespace
 }  // namespace mfd
 
+namespace mfd {
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace mfd
+
 using namespace mfd;
 
 struct mfd_handle {
@@ -159,6 +163,7 @@ struct mfd_handle {
   std::vector<int64_t> col_base, a_base;
   std::vector<int32_t> front_base;
   int64_t n_total = 0, nnz_total = 0;
+  int64_t a_len = 0;                                // length of the caller's value array (CSR input: its nnz)
   int32_t num_front = 0;
 
   // host tables
@@ -203,6 +208,7 @@ struct mfd_handle {
   int64_t launches_factor = 0, launches_solve = 0;
   double factor_ms = 0, solve_ms = 0, anorm = 0;
   double time_info[7] = {0, 0, 0, 0, 0, 0, 0};
+  double setup_s[4] = {0, 0, 0, 0};                 // analysis, plan, device index maps + exports, CSR + storage
   cudaGraphExec_t g_factor = nullptr;
   std::map<int, cudaGraphExec_t> g_solve;
 
@@ -459,6 +465,7 @@ int build_plan(mfd_handle* h) {
 }
 
 int upload_plan(mfd_handle* h) {
+  auto t0 = std::chrono::steady_clock::now();
   cudaStream_t st = h->st;
   const int32_t nfr = h->num_front;
   std::vector<int32_t> nc(nfr), nr(nfr), first(nfr), parent(nfr);
@@ -624,6 +631,8 @@ int upload_plan(mfd_handle* h) {
     }
   }
 
+  h->setup_s[2] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  t0 = std::chrono::steady_clock::now();
   // permuted full CSR (both triangles) for residuals
   {
     std::vector<int64_t> rp(h->n_total + 1, 0);
@@ -655,8 +664,10 @@ int upload_plan(mfd_handle* h) {
   CK(cudaMalloc(&h->d_diag, (size_t)std::max<int64_t>(h->dinv_elems, 1) * esz));
   // the inverted diagonal blocks are written on their lower w x w part only: the rest stays zero
   CK(cudaMemsetAsync(h->d_diag, 0, (size_t)std::max<int64_t>(h->dinv_elems, 1) * esz, h->st));
-  CK(h->d_a.alloc(h->nnz_total));
+  h->a_len = h->nnz_total;
+  CK(h->d_a.alloc(h->a_len));
   CK(h->d_norms.alloc(8));
+  h->setup_s[3] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return MFD_OK;
 }
 
@@ -1043,7 +1054,7 @@ int do_factorize(mfd_handle* h, const double* a) {
   if (!a) return fail(MFD_E_ARG, "null values");
   CK(cudaSetDevice(h->device));
   cudaMemcpyKind kind = is_device_ptr(a) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  CK(cudaMemcpyAsync(h->d_a.p, a, sizeof(double) * h->nnz_total, kind, h->st));
+  CK(cudaMemcpyAsync(h->d_a.p, a, sizeof(double) * h->a_len, kind, h->st));
   launch_fill_int(h->d_info.p + 2, h->expire_waits ? 1 : 0, 1, h->st);
   CK(cudaEventRecord(h->ev0, h->st));
   int rc = h->fp32 ? run_graph(h, &h->g_factor, [&](cudaStream_t s) { h->launches_factor = enqueue_factor<float>(h, s); })
@@ -1239,8 +1250,10 @@ int create_common(mfd_handle** out, std::vector<Symbolic>&& syms, const mfd_opti
   }
   CK(cudaEventCreate(&h->ev0));
   CK(cudaEventCreate(&h->ev1));
+  auto t0 = std::chrono::steady_clock::now();
   int rc = build_plan(h.get());
   if (rc) return rc;
+  h->setup_s[1] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   rc = upload_plan(h.get());
   if (rc) return rc;
   *out = h.release();
@@ -1286,6 +1299,27 @@ Symbolic copy_symbolic(const mfd_symbolic& s) {
 }
 
 }  // namespace
+
+namespace mfd {
+// CSR input (input.cu): the caller's values come in another order; entry k of
+// the analysed lower CCS is entry d_map[k] of the caller's array (a_len long).
+// Every value source of the handle (assembly, residual matrix) is re-pointed.
+int handle_set_value_map(mfd_handle* h, const int32_t* d_map, int64_t a_len) {
+  if (!h || h->sys.size() != 1) return fail(MFD_E_ARG, "value map: single-system handles only");
+  CK(cudaSetDevice(h->device));
+  launch_remap_int(d_map, h->d_a_src.p, h->nnz_total, h->st);
+  launch_remap_int(d_map, h->d_csr_src.p, (int64_t)h->d_csr_src.n, h->st);
+  h->a_len = a_len;
+  CK(h->d_a.alloc(a_len));
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->st));
+  for (auto& kv : h->g_solve) cudaGraphExecDestroy(kv.second);
+  h->g_solve.clear();
+  if (h->g_factor) cudaGraphExecDestroy(h->g_factor);
+  h->g_factor = nullptr;
+  return MFD_OK;
+}
+}  // namespace mfd
 
 // ==================================================================================
 // C ABI
@@ -1336,7 +1370,7 @@ int mfd_analyze(mfd_handle** h, int32_t n, const int32_t* ccs_col, const int32_t
   if (analyze(n, ccs_col, ccs_row, order_perm, o.max_zero, v[0])) return fail(MFD_E_ARG, "malformed matrix or ordering");
   double ta = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   int rc = create_common(h, std::move(v), &o);
-  if (rc == MFD_OK) (*h)->time_info[1] = ta;
+  if (rc == MFD_OK) (*h)->time_info[1] = (*h)->setup_s[0] = ta;
   return rc;
 }
 
@@ -1389,7 +1423,7 @@ int mfd_analyze_batch(mfd_handle** h, int32_t num_systems, const int32_t* n, con
     if (rcs[s]) return fail(MFD_E_ARG, "malformed matrix or ordering in system " + std::to_string(s));
   double ta = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   int rc = create_common(h, std::move(v), &o);
-  if (rc == MFD_OK) (*h)->time_info[1] = ta;
+  if (rc == MFD_OK) (*h)->time_info[1] = (*h)->setup_s[0] = ta;
   return rc;
 }
 
@@ -1463,6 +1497,7 @@ int mfd_get_stats(mfd_handle* h, mfd_stats* st) {
   st->solve_ms = h->solve_ms;
   st->pivot_fallbacks = h->pivot_fallbacks;
   std::memcpy(st->time_info, h->time_info, sizeof(st->time_info));
+  std::memcpy(st->setup_s, h->setup_s, sizeof(st->setup_s));
   return MFD_OK;
 }
 

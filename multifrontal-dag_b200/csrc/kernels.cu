@@ -2745,6 +2745,13 @@ void launch_axpy_from_t(const T* d, double* x, int64_t n, cudaStream_t st) {
 void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
   if (n > 0) k_fill_int<<<grid_1d(n), 256, 0, st>>>(p, v, n);
 }
+__global__ void k_remap_int(const int32_t* map, int32_t* a, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = map[a[i]];
+}
+void launch_remap_int(const int32_t* map, int32_t* a, int64_t n, cudaStream_t st) {
+  if (n > 0) k_remap_int<<<grid_1d(n), 256, 0, st>>>(map, a, n);
+}
 
 #define MFD_INSTANTIATE(T)                                                                                          \
   template void launch_small_fronts<T>(const DevFronts&, const int32_t*, int, int, const double*, T*, T*, int32_t*, \

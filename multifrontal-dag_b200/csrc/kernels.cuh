@@ -208,5 +208,7 @@ void launch_to_t(const double* in, T* out, int64_t n, cudaStream_t st);
 template <typename T>
 void launch_axpy_from_t(const T* d, double* x, int64_t n, cudaStream_t st);
 void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st);
+// a[i] = map[a[i]] for i < n
+void launch_remap_int(const int32_t* map, int32_t* a, int64_t n, cudaStream_t st);
 
 }  // namespace mfd

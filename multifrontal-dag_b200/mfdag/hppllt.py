@@ -42,6 +42,10 @@ class Symbolic(C.Structure):
                 ("acol_ptr", C.c_void_p), ("arow", C.c_void_p), ("ccs_perm", C.c_void_p), ("perm", C.c_void_p)]
 
 
+class Coo(C.Structure):
+    _fields_ = [("n", C.c_int32), ("nnz", C.c_int64), ("row", C.c_void_p), ("col", C.c_void_p), ("val", C.c_void_p)]
+
+
 class Report(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("backward_error", C.c_double),
                 ("residual_ref", C.c_double), ("time_ms", C.c_double)]
@@ -60,7 +64,7 @@ class Stats(C.Structure):
                 ("cost", C.c_int64), ("nonzero", C.c_int64), ("panel_bytes", C.c_int64),
                 ("update_pool_bytes", C.c_int64), ("launches_factor", C.c_int64), ("launches_solve", C.c_int64),
                 ("max_front", C.c_int64), ("factor_ms", C.c_double), ("solve_ms", C.c_double),
-                ("time_info", C.c_double * 7), ("pivot_fallbacks", C.c_int64)]
+                ("time_info", C.c_double * 7), ("pivot_fallbacks", C.c_int64), ("setup_s", C.c_double * 4)]
 
 
 EXPORTS = [
@@ -69,7 +73,9 @@ EXPORTS = [
     "mfd_solve", "mfd_factorize_solve", "mfd_get_stats", "mfd_get_index", "mfd_get_symbolic", "mfd_get_front_panel",
     "mfd_destroy", "mfd_last_error", "mfd_set_profiling", "mfd_get_profile", "mfd_test_expire_waits",
     "mfd_factor_fronts_noalloc",
-    "mfd_noalloc_last_error", "mfd_symbolic_analyze", "mfd_symbolic_view", "mfd_symbolic_free", "hppllt_init", "hppllt_set_precision", "hppllt_analyze", "hppllt_set_ordering",
+    "mfd_noalloc_last_error", "mfd_symbolic_analyze", "mfd_symbolic_view", "mfd_symbolic_free", "mfd_mm_read",
+    "mfd_coo_free", "mfd_coo_to_ccs", "mfd_analyze_csr", "hppllt_init", "hppllt_set_precision", "hppllt_analyze",
+    "hppllt_set_ordering",
     "hppllt_factorize", "hppllt_solve", "hppllt_finalize", "hppllt_get_time_info", "hppllt_get_cost",
     "hppllt_get_nonzero", "hppllt_get_array_size",
 ]
@@ -122,6 +128,11 @@ def load(build_if_missing: bool = True):
     L.mfd_symbolic_view.argtypes = [vp, C.POINTER(Symbolic)]
     L.mfd_symbolic_free.argtypes = [vp]
     L.mfd_last_error.restype = C.c_char_p
+    L.mfd_mm_read.argtypes = [C.c_char_p, C.POINTER(Coo)]
+    L.mfd_coo_free.argtypes = [C.POINTER(Coo)]
+    L.mfd_coo_free.restype = None
+    L.mfd_coo_to_ccs.argtypes = [i32, i64, vp, vp, vp, vp, vp, vp, i32]
+    L.mfd_analyze_csr.argtypes = [C.POINTER(vp), i32, vp, vp, i32, vp, C.POINTER(Options)]
     L.hppllt_init.argtypes = [vp, i32]
     L.hppllt_set_precision.argtypes = [i32]
     L.hppllt_analyze.argtypes = [vp, vp, i32]
@@ -178,6 +189,49 @@ def symbolic_analyze(n, ccs_col, ccs_row, order_perm=None, max_zero=10) -> dict:
         L.mfd_symbolic_free(a)
 
 
+def mm_read(path) -> dict:
+    """Matrix Market coordinate file (mfd_mm_read): {"n", "row", "col", "val"}, 1-based."""
+    L = load()
+    coo = Coo()
+    _check(L.mfd_mm_read(os.fsencode(path), C.byref(coo)))
+    try:
+        k = int(coo.nnz)
+
+        def arr(ptr, ct):
+            if k == 0:
+                return np.zeros(0, np.dtype(ct))
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(k,)).copy()
+
+        return {"n": int(coo.n), "row": arr(coo.row, C.c_int32), "col": arr(coo.col, C.c_int32),
+                "val": arr(coo.val, C.c_double)}
+    finally:
+        L.mfd_coo_free(C.byref(coo))
+
+
+def coo_to_ccs(n, row, col, val=None, device: int = 0):
+    """COO -> lower CCS on the GPU (mfd_coo_to_ccs): (ccs_col, ccs_row, ccs_val or None).
+    Host numpy inputs give host outputs; CUDA tensors give CUDA tensors."""
+    L = load()
+    if hasattr(row, "data_ptr"):
+        import torch
+        nnz = int(row.numel())
+        ptr = torch.empty(int(n) + 1, dtype=torch.int32, device=row.device)
+        r = torch.empty(max(nnz, 1), dtype=torch.int32, device=row.device)
+        v = torch.empty(max(nnz, 1), dtype=torch.float64, device=row.device) if val is not None else None
+        _check(L.mfd_coo_to_ccs(int(n), nnz, row.data_ptr(), col.data_ptr(), val.data_ptr() if val is not None else None,
+                                ptr.data_ptr(), r.data_ptr(), v.data_ptr() if v is not None else None, int(device)))
+        return ptr, r[:nnz], (v[:nnz] if v is not None else None)
+    row, col = _i32(row), _i32(col)
+    nnz = int(row.size)
+    ptr = np.zeros(int(n) + 1, np.int32)
+    r = np.zeros(max(nnz, 1), np.int32)
+    vv = np.ascontiguousarray(val, dtype=np.float64) if val is not None else None
+    out = np.zeros(max(nnz, 1), np.float64) if val is not None else None
+    _check(L.mfd_coo_to_ccs(int(n), nnz, row.ctypes.data, col.ctypes.data, vv.ctypes.data if vv is not None else None,
+                            ptr.ctypes.data, r.ctypes.data, out.ctypes.data if out is not None else None, int(device)))
+    return ptr, r[:nnz], (out[:nnz] if out is not None else None)
+
+
 def default_options(**kw) -> Options:
     o = Options()
     load().mfd_default_options(C.byref(o))
@@ -212,6 +266,19 @@ class Solver:
         h = C.c_void_p()
         _check(L.mfd_analyze(C.byref(h), int(n), col.ctypes.data, row.ctypes.data,
                              op.ctypes.data if op is not None else None, C.byref(o)))
+        return cls(h, int(n))
+
+    @classmethod
+    def analyze_csr(cls, n, csr_ptr, csr_col, base: int = 0, order_perm=None, **opts) -> "Solver":
+        """Symmetric matrix given as the CSR of its lower triangle or of the whole
+        matrix (mfd_analyze_csr); factorize() then takes values in CSR order."""
+        L = load()
+        o = default_options(**opts)
+        ptr, col = _i32(csr_ptr), _i32(csr_col)
+        op = _i32(order_perm) if order_perm is not None else None
+        h = C.c_void_p()
+        _check(L.mfd_analyze_csr(C.byref(h), int(n), ptr.ctypes.data, col.ctypes.data, int(base),
+                                 op.ctypes.data if op is not None else None, C.byref(o)))
         return cls(h, int(n))
 
     @classmethod

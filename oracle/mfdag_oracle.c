@@ -1424,6 +1424,44 @@ EXPORT void orc_sweep(orc_t *h, double *tmp, int backward) {
 }
 
 /* ------------------------------------------------------------------------- */
+/* the driver's COO -> CCS conversion (example.f90:95-145), step by step:     */
+/* counting sort by row (each row's entries placed from its segment's end,    */
+/* so equal rows come out in reverse input order), then a counting sort by    */
+/* column over that order taken backwards.  1-based in and out.               */
+/* ------------------------------------------------------------------------- */
+EXPORT void orc_coo_to_ccs(int n, int nnz, const int *coo_row, const int *coo_col, const double *coo_val,
+                           int *ccs_col, int *ccs_row, double *ccs_val) {
+  int *ncol = xcalloc(n + 1, sizeof(int)), *row_num = xcalloc(n + 1, sizeof(int));
+  int *tmp_row = xmalloc(sizeof(int) * (nnz ? nnz : 1)), *tmp_col = xmalloc(sizeof(int) * (nnz ? nnz : 1));
+  double *tmp_val = xmalloc(sizeof(double) * (nnz ? nnz : 1));
+  for (int i = 0; i < nnz; i++) {                                   /* 1: key counting (:110-118) */
+    if (coo_col[i] == 0) continue;
+    ncol[coo_col[i] - 1]++;
+    row_num[coo_row[i] - 1]++;
+  }
+  row_num[0] += 1;                                                  /* 2: locations (:120-127) */
+  for (int i = 1; i < n; i++) row_num[i] += row_num[i - 1];
+  ncol[0] += 1;
+  for (int i = 1; i < n; i++) ncol[i] += ncol[i - 1];
+  ccs_col[0] = 1;                                                   /* 3: set col (:129-132) */
+  for (int i = 0; i < n; i++) ccs_col[i + 1] = ncol[i];
+  for (int i = 0; i < nnz; i++) {                                   /* 4: sort by rows (:134-140) */
+    int r = coo_row[i] - 1;
+    row_num[r]--;
+    tmp_row[row_num[r] - 1] = coo_row[i];
+    tmp_col[row_num[r] - 1] = coo_col[i];
+    tmp_val[row_num[r] - 1] = coo_val[i];
+  }
+  for (int i = nnz - 1; i >= 0; i--) {                              /* 5: set row (:142-146) */
+    int c = tmp_col[i] - 1;
+    ncol[c]--;
+    ccs_row[ncol[c] - 1] = tmp_row[i];
+    ccs_val[ncol[c] - 1] = tmp_val[i];
+  }
+  free(ncol); free(row_num); free(tmp_row); free(tmp_col); free(tmp_val);
+}
+
+/* ------------------------------------------------------------------------- */
 /* unit-level entry points for the reference's algorithm tests                */
 /* ------------------------------------------------------------------------- */
 EXPORT void orc_t_compute_tree(int n, const int *crs_ptr, const int *crs_val, int *parent_out) {

@@ -59,6 +59,7 @@ def lib():
     L.orc_solve.argtypes = [vp, F64P]
     L.orc_sweep.argtypes = [vp, F64P, C.c_int]
     L.orc_solve_many.argtypes = [vp, F64P, C.c_int, C.c_int64, C.c_int]
+    L.orc_coo_to_ccs.argtypes = [C.c_int, C.c_int, I32P, I32P, F64P, I32P, I32P, F64P]
     L.orc_get_size.restype = C.c_int
     L.orc_get_size.argtypes = [vp, C.c_int]
     L.orc_get.restype = C.c_int
@@ -252,6 +253,17 @@ class Oracle:
 # ---------------------------------------------------------------------------
 # unit-level restatements used by the golden-vector tests
 # ---------------------------------------------------------------------------
+def coo_to_ccs(n, row, col, val):
+    """The reference driver's COO -> CCS (example.f90:95-145): 1-based
+    (ccs_col, ccs_row, ccs_val)."""
+    row, col, val = i32(row), i32(col), f64(val)
+    ptr = np.zeros(n + 1, np.int32)
+    rows = np.zeros(max(1, row.size), np.int32)
+    vals = np.zeros(max(1, row.size), np.float64)
+    lib().orc_coo_to_ccs(int(n), int(row.size), row, col, val, ptr, rows, vals)
+    return ptr, rows[:row.size], vals[:row.size]
+
+
 def compute_tree(num_col, col) -> np.ndarray:
     n = len(num_col)
     out = np.zeros(n, np.int32)

@@ -124,6 +124,14 @@ int mfd_create_batch(mfd_handle **h, int32_t num_systems, const mfd_symbolic *sy
 int mfd_analyze(mfd_handle **h, int32_t n, const int32_t *ccs_col, const int32_t *ccs_row,
                 const int32_t *order_perm, const mfd_options *opt);
 
+/* Fill-reducing ordering (host, no device work) where the reference calls
+ * METIS_NodeND (ordering_m.f90:11-36): nested dissection of the graph of the
+ * lower CCS (1-based, any row order), by BFS level-structure bisection with a
+ * refined separator.  order_perm (n) receives new -> old, 1-based -- the
+ * argument mfd_analyze takes.  hppllt_analyze with use_metis = 1 uses it when
+ * no ordering was supplied through hppllt_set_ordering. */
+int mfd_order(int32_t n, const int32_t *ccs_col, const int32_t *ccs_row, int32_t *order_perm);
+
 /* Host-only symbolic analysis (hppllt_analyze's symbolic half, no device work):
  * the result object owns the arrays; mfd_symbolic_view fills an mfd_symbolic
  * whose pointers stay valid until mfd_symbolic_free. */
@@ -289,7 +297,8 @@ int hppllt_init(const int32_t *options, int32_t noptions);
 /* Selects the arithmetic (MFD_PREC_*) of the next factorize; not in the reference. */
 int hppllt_set_precision(int32_t precision);
 /* hppllt_analyze(ccs_col, ccs_row, n) (hppllt.f90:24-81); with use_metis = 1 the
- * ordering must be supplied first through hppllt_set_ordering. */
+ * ordering is the one supplied through hppllt_set_ordering, or else mfd_order's
+ * nested dissection (the reference calls METIS_NodeND there). */
 int hppllt_analyze(const int32_t *ccs_col, const int32_t *ccs_row, int32_t n);
 /* Supplies the fill-reducing ordering used when use_metis = 1 (new->old, 1-based). */
 int hppllt_set_ordering(const int32_t *order_perm, int32_t n);

@@ -30,4 +30,8 @@ struct Symbolic {
 int analyze(int32_t n, const int32_t* ccs_col, const int32_t* ccs_row, const int32_t* order_perm,
             int32_t max_zero, Symbolic& out);
 
+// Nested-dissection ordering of the matrix graph (ordering.cpp): order_perm
+// (n entries) receives new -> old, 1-based.  Returns 0, or -1 on bad input.
+int nested_dissection(int32_t n, const int32_t* ccs_col, const int32_t* ccs_row, int32_t* order_perm);
+
 }  // namespace mfd

@@ -1619,14 +1619,29 @@ int hppllt_analyze(const int32_t* ccs_col, const int32_t* ccs_row, int32_t n) {
   o.max_zero = g_ref.options[1];
   o.precision = g_ref.precision;
   const int32_t* ord = nullptr;
-  if (g_ref.options[3] == 1) {
-    if ((int32_t)g_ref.order.size() != n) return fail(MFD_E_ARG, "use_metis=1 needs an ordering (hppllt_set_ordering)");
-    ord = g_ref.order.data();
-  }
+  std::vector<int32_t> nd;
   auto t0 = std::chrono::steady_clock::now();
+  if (g_ref.options[3] == 1) {
+    // use_metis = 1 (hppllt.f90:47-51): a caller-supplied ordering, else the
+    // library's nested dissection where the reference calls METIS_NodeND
+    if ((int32_t)g_ref.order.size() == n) {
+      ord = g_ref.order.data();
+    } else {
+      nd.resize(n > 0 ? n : 1);
+      if (n < 1 || nested_dissection(n, ccs_col, ccs_row, nd.data())) return fail(MFD_E_ARG, "bad matrix for ordering");
+      ord = nd.data();
+    }
+  }
+  g_ref.times[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  t0 = std::chrono::steady_clock::now();
   int rc = mfd_analyze(&g_ref.h, n, ccs_col, ccs_row, ord, &o);
   g_ref.times[1] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return rc;
+}
+
+int mfd_order(int32_t n, const int32_t* ccs_col, const int32_t* ccs_row, int32_t* order_perm) {
+  if (nested_dissection(n, ccs_col, ccs_row, order_perm)) return fail(MFD_E_ARG, "mfd_order: bad matrix");
+  return MFD_OK;
 }
 
 int hppllt_factorize(const double* a) {

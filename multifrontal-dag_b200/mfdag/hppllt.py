@@ -74,7 +74,7 @@ EXPORTS = [
     "mfd_destroy", "mfd_last_error", "mfd_set_profiling", "mfd_get_profile", "mfd_test_expire_waits",
     "mfd_factor_fronts_noalloc",
     "mfd_noalloc_last_error", "mfd_symbolic_analyze", "mfd_symbolic_view", "mfd_symbolic_free", "mfd_mm_read",
-    "mfd_coo_free", "mfd_coo_to_ccs", "mfd_analyze_csr", "hppllt_init", "hppllt_set_precision", "hppllt_analyze",
+    "mfd_coo_free", "mfd_coo_to_ccs", "mfd_analyze_csr", "mfd_order", "hppllt_init", "hppllt_set_precision", "hppllt_analyze",
     "hppllt_set_ordering",
     "hppllt_factorize", "hppllt_solve", "hppllt_finalize", "hppllt_get_time_info", "hppllt_get_cost",
     "hppllt_get_nonzero", "hppllt_get_array_size",
@@ -133,6 +133,7 @@ def load(build_if_missing: bool = True):
     L.mfd_coo_free.restype = None
     L.mfd_coo_to_ccs.argtypes = [i32, i64, vp, vp, vp, vp, vp, vp, i32]
     L.mfd_analyze_csr.argtypes = [C.POINTER(vp), i32, vp, vp, i32, vp, C.POINTER(Options)]
+    L.mfd_order.argtypes = [i32, vp, vp, vp]
     L.hppllt_init.argtypes = [vp, i32]
     L.hppllt_set_precision.argtypes = [i32]
     L.hppllt_analyze.argtypes = [vp, vp, i32]
@@ -187,6 +188,14 @@ def symbolic_analyze(n, ccs_col, ccs_row, order_perm=None, max_zero=10) -> dict:
                 "perm": arr(v.perm, v.n)}
     finally:
         L.mfd_symbolic_free(a)
+
+
+def order(n, ccs_col, ccs_row) -> np.ndarray:
+    """Nested-dissection ordering of the lower CCS (mfd_order): new -> old, 1-based."""
+    col, row = _i32(ccs_col), _i32(ccs_row)
+    out = np.zeros(int(n), np.int32)
+    _check(load().mfd_order(int(n), col.ctypes.data, row.ctypes.data, out.ctypes.data))
+    return out
 
 
 def mm_read(path) -> dict:

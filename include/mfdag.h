@@ -199,10 +199,13 @@ int mfd_get_stats(mfd_handle *h, mfd_stats *st);
 
 /* Autotuner (no counterpart in the reference): times the factorization of the
  * values `a` (host or device pointer, as for mfd_factorize) under candidate
- * settings of the knobs that shape the schedule -- the small-front / blocked
- * split small_front_max in {32, 64, 96, 128} and the lookahead on / off --
- * each on a temporary handle built from h's symbolic data (one warm-up, then
- * the median of `repeats` timed factorizations).  Writes the fastest options
+ * settings, each on a temporary handle built from h's symbolic data (one
+ * warm-up, then the median of `repeats` timed factorizations).  Stage 1: the
+ * schedule -- the small-front / blocked split small_front_max in
+ * {32, 64, 96, 128} and the lookahead on / off.  Stage 2, at the best
+ * schedule: the trailing-update kernel (reserved[0]: FP64 DMMA in 128 x 64
+ * halves, whole 128 x 128 tiles, or FFMA tiles; FP32 3xTF32 tcgen05 or FFMA)
+ * and the deferral depth reserved[5] in {1, 2}.  Writes the fastest options
  * to *best and their factor time (ms) to *best_ms; h is left unchanged: create
  * a handle with *best to use them.  Returns a pivot column > 0 if a
  * factorization fails. */

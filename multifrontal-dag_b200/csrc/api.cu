@@ -1439,34 +1439,63 @@ int mfd_solve(mfd_handle* h, double* b, int32_t nrhs, int64_t ldb, mfd_report* r
 
 int mfd_autotune(mfd_handle* h, const double* a, int32_t repeats, mfd_options* best, double* best_ms) {
   if (!h || !a || !best || repeats < 1) return fail(MFD_E_ARG, "autotune: null handle, values or output");
-  const int sfms[] = {32, 64, 96, 128};   // small-front split (at most kSmallFrontMax)
   double best_t = 1e300;
   mfd_options best_o = h->opt;
-  for (int sfm : sfms) {
+  // one candidate: a temporary handle on h's symbolic data, one warm-up
+  // factorization (graph capture), then the median of `repeats`
+  auto trial = [&](const mfd_options& o, int* err) -> double {
+    std::vector<Symbolic> syms = h->sys;
+    mfd_handle* t = nullptr;
+    if (create_common(&t, std::move(syms), &o) != MFD_OK) return 1e300;   // e.g. out of memory: skip it
+    std::unique_ptr<mfd_handle> guard(t);
+    int rc = do_factorize(t, a);
+    if (rc != MFD_OK) { *err = rc; return 1e300; }
+    std::vector<double> ms;
+    for (int r = 0; r < repeats; ++r) {
+      rc = do_factorize(t, a);
+      if (rc != MFD_OK) { *err = rc; return 1e300; }
+      ms.push_back(t->factor_ms);
+    }
+    std::sort(ms.begin(), ms.end());
+    return ms[ms.size() / 2];
+  };
+  auto consider = [&](const mfd_options& o) -> int {
+    int err = MFD_OK;
+    const double t = trial(o, &err);
+    if (err != MFD_OK) return err;
+    if (t < best_t) {
+      best_t = t;
+      best_o = o;
+    }
+    return MFD_OK;
+  };
+  // stage 1: the schedule -- small-front / blocked split x lookahead
+  const int sfms[] = {32, 64, 96, 128};   // small-front split (at most kSmallFrontMax)
+  for (int sfm : sfms)
     for (int lookahead_off = 0; lookahead_off <= 1; ++lookahead_off) {
       mfd_options o = h->opt;
       o.small_front_max = sfm;
       o.reserved[1] = lookahead_off;
-      std::vector<Symbolic> syms = h->sys;
-      mfd_handle* t = nullptr;
-      if (create_common(&t, std::move(syms), &o) != MFD_OK) continue;   // e.g. out of memory: skip the candidate
-      std::unique_ptr<mfd_handle> guard(t);
-      int rc = do_factorize(t, a);                                      // warm-up (captures the graph)
-      if (rc != MFD_OK) return rc;
-      std::vector<double> ms;
-      for (int r = 0; r < repeats; ++r) {
-        rc = do_factorize(t, a);
-        if (rc != MFD_OK) return rc;
-        ms.push_back(t->factor_ms);
-      }
-      std::sort(ms.begin(), ms.end());
-      const double med = ms[ms.size() / 2];
-      if (med < best_t) {
-        best_t = med;
-        best_o = o;
-      }
+      int rc = consider(o);
+      if (rc) return rc;
     }
-  }
+  // stage 2, at the best schedule: the trailing-update kernel (FP64: DMMA in
+  // 128 x 64 halves / whole 128 x 128 tiles / FFMA; FP32: 3xTF32 tcgen05 /
+  // FFMA) and the deferral depth of the bulk update (1, 2 panel steps)
+  const mfd_options base = best_o;
+  const bool fp32 = base.precision == MFD_PREC_FP32_IR;
+  const int kinds64[] = {0, 3, 1}, kinds32[] = {0, 1};
+  const int* kinds = fp32 ? kinds32 : kinds64;
+  const int nk = fp32 ? 2 : 3;
+  for (int ki = 0; ki < nk; ++ki)
+    for (int d = 1; d <= 2; ++d) {
+      mfd_options o = base;
+      o.reserved[0] = kinds[ki];
+      o.reserved[5] = d;
+      if (kinds[ki] == base.reserved[0] && d == std::max(1, base.reserved[5])) continue;   // timed in stage 1
+      int rc = consider(o);
+      if (rc) return rc;
+    }
   *best = best_o;
   if (best_ms) *best_ms = best_t;
   return MFD_OK;

@@ -292,6 +292,7 @@ def test_autotune_picks_a_candidate():
     s = gpu_for(p, max_zero=1000)
     opts, ms = s.autotune(p.val, repeats=1)
     assert opts["small_front_max"] in (32, 64, 96, 128) and ms > 0
+    assert opts["reserved"][0] in (0, 1, 3) and opts["reserved"][5] in (0, 1, 2)
     t = gpu_for(p, max_zero=1000, **opts)
     x = p.rhs.copy()
     rep, rc = t.solve(x)

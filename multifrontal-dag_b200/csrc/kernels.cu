@@ -1117,8 +1117,8 @@ __global__ void __launch_bounds__(kUThreads, 1) k_update_dmma(DevFronts F, const
 // (rows) x 2 (columns) of 32 x 32, each 2 x 4 mma.m16n8k16.f64 per K step of
 // 16, so 128 registers and 102 KB of shared memory per CTA and two CTAs per
 // SM: one CTA's C loads and stores overlap the other's MMAs.  Operands come
-// in K chunks of 32 by cp.async, double-buffered; a diagonal tile's B is rows
-// 64 h .. of its A.  C is loaded into the accumulators (the A fragments enter
+// in K chunks of 32 by cp.async (16-byte row pairs where aligned),
+// double-buffered; a diagonal tile's B is rows 64 h .. of its A.  C is loaded into the accumulators (the A fragments enter
 // negated) and stored back; tiles wholly inside the trailing matrix, below
 // the diagonal and inside the panel or the update matrix take an unchecked
 // path.  In a diagonal tile's right half the warps whose 32 rows all lie
@@ -1154,25 +1154,50 @@ __global__ void __launch_bounds__(kU2Threads, 2) k_update_dmma2(DevFronts F, con
   double* P = panel + F.panel_off[f];
   double* U = upool + F.u_off[f];
   const int nchunks = (K + kUK - 1) / kUK;
-  auto load = [&](int stage, int kc) {
-    double* dst = sm + stage * kU2Stage;
-    const int ne = diag ? kUK * kUT : kUK * (kUT + kU2N);    // a diagonal tile's B is in A
-    for (int e = threadIdx.x; e < ne; e += kU2Threads) {
-      int k, row;
-      double* d;
-      if (e < kUK * kUT) {
-        k = e >> 7; const int r = e & (kUT - 1);
-        row = i0 + r; d = dst + k * kULD + r;
-      } else {
-        const int e2 = e - kUK * kUT;
-        k = e2 >> 6; const int r = e2 & (kU2N - 1);
-        row = j0 + r; d = dst + kUK * kULD + k * kU2LdB + r;
-      }
-      const int col = kc * kUK + k;
-      const bool valid = row < nf && col < K;
-      cp_async8(d, valid ? P + row + (size_t)(kbeg + col) * nf : P, valid);
+  // Copies: thread t moves row pairs -- A rows i0 + 2 (t & 63) (+1) at columns
+  // (t >> 6) + 4 v, v < 8; B rows j0 + 2 (t & 31) (+1) at columns (t >> 5) +
+  // 8 v, v < 4 (a diagonal tile's B is in A) -- 16 bytes per copy when the
+  // pair's source is 16-byte aligned.  A thread's copies are 4 or 8 columns
+  // apart, so the alignment is the same for all of them (and, the lanes of a
+  // warp sharing the column, the same across the warp); otherwise two 8-byte
+  // copies.  Rows past the matrix and columns past K are zero-filled.
+  auto copy = [&](double* d, const double* src, int bytes, bool al) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(d);
+    if (al) {
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(bytes ? src : P), "r"(bytes));
+    } else {
+      const int b0 = bytes >= 8 ? 8 : 0, b1 = bytes >= 16 ? 8 : 0;
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(b0 ? src : P), "r"(b0));
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa + 8), "l"(b1 ? src + 1 : P), "r"(b1));
     }
-    cp_async_commit();
+  };
+  auto load = [&](int stage, int kc) {
+    // the per-thread quantities are recomputed here (kept live they would spill)
+    const int pa = threadIdx.x & 63, ka = threadIdx.x >> 6;
+    const int ra = i0 + 2 * pa;
+    const int na = ra < nf ? (ra + 1 < nf ? 16 : 8) : 0;          // bytes of the A pair inside the matrix
+    const bool ala = ((ra + (long long)(kbeg + ka) * nf) & 1) == 0; // panel offsets are multiples of 32 elements
+    double* dst = sm + stage * kU2Stage;
+    const int k0 = kc * kUK;
+    const double* sa = P + ra + (size_t)(kbeg + k0 + ka) * nf;
+    double* da = dst + ka * kULD + 2 * pa;
+#pragma unroll 1
+    for (int v = 0; v < 8; ++v) {                   // rolled: unrolled, the copies' addresses would be kept live
+      const int k = k0 + ka + 4 * v;
+      copy(da + v * 4 * kULD, sa + (size_t)(4 * v) * nf, k < K ? na : 0, ala);
+    }
+    if (diag) return;
+    const int pb = threadIdx.x & 31, kb = threadIdx.x >> 5;
+    const int rb = j0 + 2 * pb;
+    const int nbb = rb < nf ? (rb + 1 < nf ? 16 : 8) : 0;
+    const bool alb = ((rb + (long long)(kbeg + kb) * nf) & 1) == 0;
+    const double* sb = P + rb + (size_t)(kbeg + k0 + kb) * nf;
+    double* db = dst + kUK * kULD + kb * kU2LdB + 2 * pb;
+#pragma unroll 1
+    for (int v = 0; v < 4; ++v) {
+      const int k = k0 + kb + 8 * v;
+      copy(db + v * 8 * kU2LdB, sb + (size_t)(8 * v) * nf, k < K ? nbb : 0, alb);
+    }
   };
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = warp >> 1, wn = warp & 1;
@@ -1181,14 +1206,19 @@ __global__ void __launch_bounds__(kU2Threads, 2) k_update_dmma2(DevFronts F, con
   // warps of a diagonal tile's right half whose rows all lie above the diagonal
   const bool idle = i0 + wm * 32 + 31 < j0 + wn * 32;
   // unchecked path: the tile is inside the trailing matrix, wholly below the
-  // diagonal and wholly in the panel or wholly in the update matrix
-  const bool full = i0 + kUT <= nf && j0 + kU2N <= nf && i0 >= j0 + kU2N && (j0 + kU2N <= nc || j0 >= nc);
-  const int ldc = j0 < nc ? nf : nr;
-  double* Cb = j0 < nc ? P + (size_t)j0 * nf : U + (size_t)(j0 - nc) * nr - nc;   // C(gi, gj) = Cb[gi + (gj - j0) ldc]
+  // diagonal and wholly in the panel or wholly in the update matrix (formed
+  // again for the epilogue rather than kept live through the K loop)
+  auto full_tile = [&]() { return i0 + kUT <= nf && j0 + kU2N <= nf && i0 >= j0 + kU2N && (j0 + kU2N <= nc || j0 >= nc); };
+  auto c_base = [&]() { return j0 < nc ? P + (size_t)j0 * nf : U + (size_t)(j0 - nc) * nr - nc; };   // C(gi, gj) = Cb[gi + (gj - j0) ldc]
   pdl_wait();
   pdl_trigger();
   load(0, 0);
+  cp_async_commit();
   double acc[2][4][4];
+  {
+  const bool full = full_tile();
+  const int ldc = j0 < nc ? nf : nr;
+  double* Cb = c_base();
 #pragma unroll
   for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -1201,9 +1231,11 @@ __global__ void __launch_bounds__(kU2Threads, 2) k_update_dmma2(DevFronts F, con
         else
           acc[mi][ni][e] = (!idle && gi < nf && gj < nf && gi >= gj) ? *trailing_addr(P, U, nc, nr, nf, gi, gj) : 0.0;
       }
+  }
   for (int kc = 0; kc < nchunks; ++kc) {
     if (kc + 1 < nchunks) {
       load((kc + 1) & 1, kc + 1);
+      cp_async_commit();
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
@@ -1233,6 +1265,9 @@ __global__ void __launch_bounds__(kU2Threads, 2) k_update_dmma2(DevFronts F, con
     __syncthreads();
   }
   if (idle) return;
+  const bool full = full_tile();
+  const int ldc = j0 < nc ? nf : nr;
+  double* Cb = c_base();
 #pragma unroll
   for (int mi = 0; mi < 2; ++mi)
 #pragma unroll

@@ -132,6 +132,19 @@ int mfd_analyze(mfd_handle **h, int32_t n, const int32_t *ccs_col, const int32_t
  * no ordering was supplied through hppllt_set_ordering. */
 int mfd_order(int32_t n, const int32_t *ccs_col, const int32_t *ccs_row, int32_t *order_perm);
 
+/* Subtree-to-GPU mapping of one system (host): the reference's tree_pruning
+ * (src/main/algorithms/tree_pruning_m.f90:13-155), restated.  Inputs are the
+ * supernodal tree as the reference holds it: node_size (supernode columns),
+ * cc (update rows nr), num_child and the concatenated children (tree_child),
+ * all 1-based, nodes in postorder with the root last.  Subtrees are split,
+ * heaviest first (weight = sum over the subtree of sum_{k=nr+1}^{nr+nc} k^2),
+ * until their weights pack into p or more bins with min / max > tol.  roots
+ * (capacity num_node) receives the subtree roots in the reference's list
+ * order and *count their number.  64-bit weights (no overflow for large
+ * fronts). */
+int mfd_subtree_partition(int32_t num_node, const int32_t *node_size, const int32_t *cc, const int32_t *num_child,
+                          const int32_t *child, double tol, int32_t p, int32_t *roots, int32_t *count);
+
 /* Host-only symbolic analysis (hppllt_analyze's symbolic half, no device work):
  * the result object owns the arrays; mfd_symbolic_view fills an mfd_symbolic
  * whose pointers stay valid until mfd_symbolic_free. */

@@ -3,7 +3,8 @@
     python multifrontal-dag_b200/build.py [--debug]
 
 Sources: csrc/analysis.cpp (host symbolic analysis), csrc/ordering.cpp (nested
-dissection ordering), csrc/kernels.cu (device
+dissection ordering), csrc/partition.cpp (subtree-to-GPU mapping),
+csrc/kernels.cu (device
 kernels), csrc/update_tc.cu (FP32 tcgen05 update), csrc/api.cu (C ABI, plan,
 launch sequences), csrc/noalloc.cu (allocation-free fronts), csrc/input.cu
 (Matrix Market, COO -> CCS on the GPU, CSR input).  Output:
@@ -18,7 +19,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "mfdag", "libmfdag.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["analysis.cpp", "ordering.cpp", "kernels.cu", "update_tc.cu", "api.cu", "noalloc.cu", "input.cu"]
+SOURCES = ["analysis.cpp", "ordering.cpp", "partition.cpp", "kernels.cu", "update_tc.cu", "api.cu", "noalloc.cu",
+           "input.cu"]
 
 
 def build(debug: bool = False, verbose: bool = False) -> str:

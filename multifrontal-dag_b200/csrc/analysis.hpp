@@ -34,4 +34,9 @@ int analyze(int32_t n, const int32_t* ccs_col, const int32_t* ccs_row, const int
 // (n entries) receives new -> old, 1-based.  Returns 0, or -1 on bad input.
 int nested_dissection(int32_t n, const int32_t* ccs_col, const int32_t* ccs_row, int32_t* order_perm);
 
+// Subtree partition of the supernodal tree for p workers (partition.cpp, the
+// reference's tree_pruning): subtree roots (1-based) in list order; empty on bad input.
+std::vector<int32_t> subtree_partition(int32_t num_node, const int32_t* node_size, const int32_t* cc,
+                                       const int32_t* num_child, const int32_t* child, double tol, int32_t p);
+
 }  // namespace mfd

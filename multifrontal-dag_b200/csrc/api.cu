@@ -1668,6 +1668,17 @@ int hppllt_analyze(const int32_t* ccs_col, const int32_t* ccs_row, int32_t n) {
   return rc;
 }
 
+int mfd_subtree_partition(int32_t num_node, const int32_t* node_size, const int32_t* cc, const int32_t* num_child,
+                          const int32_t* child, double tol, int32_t p, int32_t* roots, int32_t* count) {
+  if (!node_size || !cc || !num_child || (!child && num_node > 1) || !roots || !count)
+    return fail(MFD_E_ARG, "mfd_subtree_partition: null argument");
+  std::vector<int32_t> r = subtree_partition(num_node, node_size, cc, num_child, child, tol, p);
+  if (r.empty()) return fail(MFD_E_ARG, "mfd_subtree_partition: bad tree or p < 1");
+  std::memcpy(roots, r.data(), sizeof(int32_t) * r.size());
+  *count = (int32_t)r.size();
+  return MFD_OK;
+}
+
 int mfd_order(int32_t n, const int32_t* ccs_col, const int32_t* ccs_row, int32_t* order_perm) {
   if (nested_dissection(n, ccs_col, ccs_row, order_perm)) return fail(MFD_E_ARG, "mfd_order: bad matrix");
   return MFD_OK;

@@ -74,7 +74,7 @@ EXPORTS = [
     "mfd_destroy", "mfd_last_error", "mfd_set_profiling", "mfd_get_profile", "mfd_test_expire_waits",
     "mfd_factor_fronts_noalloc",
     "mfd_noalloc_last_error", "mfd_symbolic_analyze", "mfd_symbolic_view", "mfd_symbolic_free", "mfd_mm_read",
-    "mfd_coo_free", "mfd_coo_to_ccs", "mfd_analyze_csr", "mfd_order", "hppllt_init", "hppllt_set_precision", "hppllt_analyze",
+    "mfd_coo_free", "mfd_coo_to_ccs", "mfd_analyze_csr", "mfd_order", "mfd_subtree_partition", "hppllt_init", "hppllt_set_precision", "hppllt_analyze",
     "hppllt_set_ordering",
     "hppllt_factorize", "hppllt_solve", "hppllt_finalize", "hppllt_get_time_info", "hppllt_get_cost",
     "hppllt_get_nonzero", "hppllt_get_array_size",
@@ -134,6 +134,7 @@ def load(build_if_missing: bool = True):
     L.mfd_coo_to_ccs.argtypes = [i32, i64, vp, vp, vp, vp, vp, vp, i32]
     L.mfd_analyze_csr.argtypes = [C.POINTER(vp), i32, vp, vp, i32, vp, C.POINTER(Options)]
     L.mfd_order.argtypes = [i32, vp, vp, vp]
+    L.mfd_subtree_partition.argtypes = [i32, vp, vp, vp, vp, C.c_double, i32, vp, vp]
     L.hppllt_init.argtypes = [vp, i32]
     L.hppllt_set_precision.argtypes = [i32]
     L.hppllt_analyze.argtypes = [vp, vp, i32]
@@ -196,6 +197,29 @@ def order(n, ccs_col, ccs_row) -> np.ndarray:
     out = np.zeros(int(n), np.int32)
     _check(load().mfd_order(int(n), col.ctypes.data, row.ctypes.data, out.ctypes.data))
     return out
+
+
+def subtree_partition(node_size, cc, num_child, child, tol: float, p: int) -> list:
+    """Subtree roots (1-based, the reference's list order) for p workers (mfd_subtree_partition)."""
+    ns, c, nch = _i32(node_size), _i32(cc), _i32(num_child)
+    ch = _i32(child) if len(child) else np.zeros(1, np.int32)
+    roots = np.zeros(max(1, ns.size), np.int32)
+    cnt = np.zeros(1, np.int32)
+    _check(load().mfd_subtree_partition(int(ns.size), ns.ctypes.data, c.ctypes.data, nch.ctypes.data, ch.ctypes.data,
+                                        float(tol), int(p), roots.ctypes.data, cnt.ctypes.data))
+    return roots[:int(cnt[0])].tolist()
+
+
+def tree_of(sym: dict):
+    """(node_size, cc, num_child, child) of an analysed system's supernodal tree
+    (children ascending, as the reference's tree_child)."""
+    nn = int(sym["num_node"])
+    node_size = np.diff(sym["node_ptr"]).astype(np.int32)
+    cc = np.diff(sym["lptr"]).astype(np.int32)
+    parent = np.asarray(sym["parent"])
+    num_child = np.bincount(parent[parent > 0] - 1, minlength=nn).astype(np.int32)
+    child = (np.argsort(parent, kind="stable")[np.sum(parent == 0):] + 1).astype(np.int32)
+    return node_size, cc, num_child, child
 
 
 def mm_read(path) -> dict:

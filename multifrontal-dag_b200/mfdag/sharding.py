@@ -1,4 +1,5 @@
-"""Multi-GPU partition of a batch of independent systems.
+"""Multi-GPU partitions: a batch of independent systems, and the subtrees of
+one system.
 
 A batch shards naturally: every system is factored and solved on one GPU, with
 no data-path collective (each rank owns its systems' fronts, values and
@@ -37,3 +38,24 @@ def shard_lpt(costs, world: int) -> list[list[int]]:
         parts[r].append(i)
         load[r] += costs[i]
     return [sorted(p) for p in parts]
+
+
+def subtree_weights(node_size, cc, num_child, child) -> list[int]:
+    """Subtree weight of every supernode (1-based order): the sum over its
+    subtree of sum_{k=nr+1}^{nr+nc} k^2 (tree_pruning_m.f90:75-109)."""
+    ns = np.asarray(node_size, np.int64)
+    nr = np.asarray(cc, np.int64)
+    s = lambda m: m * (m + 1) * (2 * m + 1) // 6
+    w = [int(x) for x in (s(ns + nr) - s(nr))]
+    ptr = np.concatenate([[0], np.cumsum(num_child)])
+    for i in range(len(w)):                      # children precede parents
+        for k in range(ptr[i], ptr[i + 1]):
+            w[i] += w[int(child[k]) - 1]
+    return w
+
+
+def assign_subtrees(weights, world: int) -> list[list[int]]:
+    """Subtrees (by weight) to ranks: the LPT packing tree_pruning balances
+    (heaviest first into the lightest rank, ties to the lower rank); returns
+    the ascending subtree indices of every rank."""
+    return shard_lpt(weights, world)

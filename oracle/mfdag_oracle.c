@@ -1424,6 +1424,66 @@ EXPORT void orc_sweep(orc_t *h, double *tmp, int backward) {
 }
 
 /* ------------------------------------------------------------------------- */
+/* tree_pruning (src/main/algorithms/tree_pruning_m.f90:13-155): subtree     */
+/* roots for p workers; 64-bit weights.  roots needs num_node entries.       */
+/* Returns the root count (0: bad input).                                    */
+/* ------------------------------------------------------------------------- */
+static int tp_len(const int *nx, int head) { int c = 0; for (int v = head; v; v = nx[v]) c++; return c; }
+EXPORT int orc_tree_pruning(int nn, const int *node_size, const int *cc, const int *num_child, const int *child,
+                            double tol, int p, int *roots) {
+  if (nn < 1 || p < 1) return 0;
+  int64_t *cptr = xcalloc(nn + 1, sizeof(int64_t)), *wt = xcalloc(nn + 1, sizeof(int64_t));
+  for (int i = 0; i < nn; i++) cptr[i + 1] = cptr[i] + num_child[i];
+  for (int i = 1; i <= nn; i++) {                        /* count_op_count + generate_tree_weights (:75-109) */
+    int64_t l = cc[i - 1], k = node_size[i - 1] + l;
+    wt[i] = k * (k + 1) * (2 * k + 1) / 6 - l * (l + 1) * (2 * l + 1) / 6;
+    for (int64_t q = cptr[i - 1]; q < cptr[i]; q++) wt[i] += wt[child[q]];
+  }
+  int *nx = xcalloc(nn + 1, sizeof(int)), *pv = xcalloc(nn + 1, sizeof(int));
+  int64_t *bins = xmalloc(sizeof(int64_t) * (nn + 2)), *w = xmalloc(sizeof(int64_t) * (nn + 1));
+  int count = 0;
+  for (;;) {
+    memset(nx, 0, sizeof(int) * (nn + 1)); memset(pv, 0, sizeof(int) * (nn + 1));
+    int head = nn;                                       /* call subtree_list%add(n) */
+    double ratio = 0.0;
+    int ip = p - 1, stuck = 0;
+    while (ratio <= tol) {                               /* :38-61 */
+      ip++;
+      while (tp_len(nx, head) < ip) {                    /* partition_tree (:111-132) */
+        int best = 0; int64_t bw = 0;
+        for (int v = head; v; v = nx[v]) if (wt[v] > bw) { bw = wt[v]; best = v; }   /* find_node_with_max_op */
+        if (!best) { stuck = 1; break; }
+        for (int64_t q = cptr[best - 1]; q < cptr[best]; q++) {   /* add: at the head */
+          int c = child[q];
+          if (head) pv[head] = c;
+          nx[c] = head; head = c; pv[c] = 0;
+        }
+        int a = nx[best], b = pv[best];                  /* remove */
+        if (!b) head = a; else nx[b] = a;
+        if (a) pv[a] = b;
+      }
+      if (stuck) break;
+      int m = 0;                                         /* LPT over ip bins (op max-heap, bin min-heap) */
+      for (int v = head; v; v = nx[v]) w[m++] = wt[v];
+      for (int i = 0; i < ip; i++) bins[i] = 0;
+      for (int t = 0; t < m; t++) {
+        int imax = 0; for (int i = 1; i < m; i++) if (w[i] > w[imax]) imax = i;
+        int imin = 0; for (int i = 1; i < ip; i++) if (bins[i] < bins[imin]) imin = i;
+        bins[imin] += w[imax]; w[imax] = -1;
+      }
+      int64_t mn = bins[0], mx = bins[0];
+      for (int i = 1; i < ip; i++) { if (bins[i] < mn) mn = bins[i]; if (bins[i] > mx) mx = bins[i]; }
+      ratio = mx > 0 ? (double)mn / (double)mx : 0.0;
+    }
+    if (stuck && !(ip - 1 < 1 || (tol == 0.0 && ip - 1 == p))) { tol = 0.0; p = ip - 1; continue; }   /* :46-50 */
+    for (int v = head; v; v = nx[v]) roots[count++] = v;
+    break;
+  }
+  free(cptr); free(wt); free(nx); free(pv); free(bins); free(w);
+  return count;
+}
+
+/* ------------------------------------------------------------------------- */
 /* the driver's COO -> CCS conversion (example.f90:95-145), step by step:     */
 /* counting sort by row (each row's entries placed from its segment's end,    */
 /* so equal rows come out in reverse input order), then a counting sort by    */

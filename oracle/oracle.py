@@ -60,6 +60,8 @@ def lib():
     L.orc_sweep.argtypes = [vp, F64P, C.c_int]
     L.orc_solve_many.argtypes = [vp, F64P, C.c_int, C.c_int64, C.c_int]
     L.orc_coo_to_ccs.argtypes = [C.c_int, C.c_int, I32P, I32P, F64P, I32P, I32P, F64P]
+    L.orc_tree_pruning.restype = C.c_int
+    L.orc_tree_pruning.argtypes = [C.c_int, I32P, I32P, I32P, I32P, C.c_double, C.c_int, I32P]
     L.orc_get_size.restype = C.c_int
     L.orc_get_size.argtypes = [vp, C.c_int]
     L.orc_get.restype = C.c_int
@@ -262,6 +264,15 @@ def coo_to_ccs(n, row, col, val):
     vals = np.zeros(max(1, row.size), np.float64)
     lib().orc_coo_to_ccs(int(n), int(row.size), row, col, val, ptr, rows, vals)
     return ptr, rows[:row.size], vals[:row.size]
+
+
+def tree_pruning(node_size, cc, num_child, child, tol, p) -> list:
+    """tree_pruning_m.f90:13-155: subtree roots (1-based) for p workers."""
+    ns = i32(node_size)
+    roots = np.zeros(max(1, ns.size), np.int32)
+    ch = i32(child) if len(child) else np.zeros(1, np.int32)
+    k = lib().orc_tree_pruning(int(ns.size), ns, i32(cc), i32(num_child), ch, float(tol), int(p), roots)
+    return roots[:k].tolist()
 
 
 def compute_tree(num_col, col) -> np.ndarray:

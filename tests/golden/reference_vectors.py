@@ -34,9 +34,20 @@ SN_TREE_CHILD_VAL = [1, 4, 3, 5, 2, 6]                          # :43
 POST_PERM = [1, 7, 2, 4, 3, 5, 6, 8, 9]                         # perm_maker_m.f90:7
 POST_IPERM = [1, 3, 5, 4, 6, 7, 2, 8, 9]                        # :11
 
+# supernodal 7-node fixture of tree_pruning_test.f90: nr and node sizes
+SN_CC = [2, 2, 2, 2, 2, 2, 0]                                    # src/test_mod/sparse_matrix_maker_m.f90:88
+SN_NODE_SIZE = [1, 1, 2, 1, 1, 1, 2]                             # src/test_mod/sparse_matrix_maker_m.f90:96
+
 # ---------------------------------------------------------------------------
 # algorithm tests
 # ---------------------------------------------------------------------------
+# tree_pruning_test.f90:23-33: (tol, p) -> subtree roots in list order
+TREE_PRUNING_P1 = [7]                                            # src/test/algorithms/tree_pruning_test.f90:24
+TREE_PRUNING_P2 = [6, 2]                                         # src/test/algorithms/tree_pruning_test.f90:27
+TREE_PRUNING_TOL071 = [5, 3, 2]                                  # src/test/algorithms/tree_pruning_test.f90:30
+TREE_PRUNING_TOL073 = [5, 3, 2]                                  # src/test/algorithms/tree_pruning_test.f90:33
+TREE_PRUNING_CASES = [(0.0, 1, TREE_PRUNING_P1), (0.0, 2, TREE_PRUNING_P2), (0.71, 2, TREE_PRUNING_TOL071),
+                      (0.73, 2, TREE_PRUNING_TOL073)]
 COLUMN_COUNT = [3, 3, 4, 3, 3, 3, 3, 2, 1]                      # src/test/algorithms/column_count_test.f90:17
 FINDING_LEAVES_SUBTREE = [1, 2, 1, 2, 1, 2, 5, 8, 9]            # finding_leaves_test.f90:13
 FINDING_LEAVES = [1, 1, 1, 0, 1, 1, 0, 0, 0]                    # :15

@@ -1718,3 +1718,181 @@ EXPORT int orc_factorize_parallel(orc_t *h, const double *a, int nthreads) {
   return h->info;
 }
 EXPORT int orc_max_threads(void) { return (int)sysconf(_SC_NPROCESSORS_ONLN); }
+
+/* ------------------------------------------------------------------------- */
+/* CPU baseline with the reference's DAG schedule: starpu_factorize_m.f90     */
+/* :13-101 submits one StarPU task per tile operation in the sequential loop  */
+/* order and lets StarPU order them by each task's access modes on the tiles  */
+/* (R, RW, RW|COMMUTE: factorize_tasks_m.f90:12-15, border_tasks_m.f90:12-13, */
+/* rearrange_tasks_m.f90:12-13, extend_add_tasks_m.f90:12-13).  Here the same */
+/* operations go out in the same order as OpenMP tasks whose depend clauses   */
+/* restate those modes on the tiles' addresses: R -> in, RW -> inout,         */
+/* RW|COMMUTE -> mutexinoutset (the children's extend-adds into one parent    */
+/* tile, in any order, one at a time).  Each task calls the sequential BLAS   */
+/* (the reference links -mkl=sequential).  Assembly is an OpenMP loop over    */
+/* supernodes, as in zero_setter_m.f90:18 and coefficient_setter_m.f90:25.    */
+/* ------------------------------------------------------------------------- */
+static void dag_supernode(factors_t *f, int node, int *res);
+static void dag_note(int *res, int node, int r) {
+  if (!r) return;
+  #pragma omp critical(orc_dag_info)
+  { if (!res[node - 1] || r < res[node - 1]) res[node - 1] = r; }
+}
+static void dag_border(factors_t *f, int node, int *res) {                     /* seq_factorize_m.f90:54-79 as tasks */
+  nd_t *d = f->nd;
+  int j = nd_work_start(d, node), nbk = nd_num_matrix_block(d, node), nb = d->nb;
+  int ss = d->ss[node - 1], ws = d->ws[node - 1];
+  double *bjj = f_matrix(f, node, j, j), *sjj = f_sup(f, node, j, j), *wjj = f_work(f, node, j, j);
+  #pragma omp task depend(in: bjj[0]) depend(inout: sjj[0], wjj[0]) firstprivate(bjj, sjj, wjj, ss, ws)
+  { /* rearrange_diag -> split_tri_matrix (matrix_splitter_m.f90:5-28) */
+    int lo = ss + ws;
+    for (int i = 1; i <= ss; i++) for (int jj = 1; jj <= i; jj++) sjj[(jj - 1) + (int64_t)(i - 1) * ss] = bjj[(jj - 1) + (int64_t)(i - 1) * lo];
+    for (int i = ss + 1; i <= ss + ws; i++) for (int jj = 1; jj <= ss; jj++) sjj[(jj - 1) + (int64_t)(i - 1) * ss] = bjj[(jj - 1) + (int64_t)(i - 1) * lo];
+    for (int i = 1; i <= ws; i++) for (int jj = 1; jj <= i; jj++) wjj[(jj - 1) + (int64_t)(i - 1) * ws] = bjj[(jj + ss - 1) + (int64_t)(i + ss - 1) * lo];
+  }
+  for (int i = j + 1; i <= nbk; i++) { /* rearrange_ndiag -> split_rect_matrix (:30-46) */
+    double *o = f_matrix(f, node, i, j), *l = f_sup(f, node, i, j), *r = f_work(f, node, i, j);
+    int nrow = nd_msize(d, i, node);
+    #pragma omp task depend(in: o[0]) depend(inout: l[0], r[0]) firstprivate(o, l, r, nrow, ss, ws)
+    {
+      int lo = ss + ws;
+      for (int ii = 0; ii < nrow; ii++) {
+        for (int jj = 0; jj < ss; jj++) l[jj + (int64_t)ii * ss] = o[jj + (int64_t)ii * lo];
+        for (int jj = 0; jj < ws; jj++) r[jj + (int64_t)ii * ws] = o[ss + jj + (int64_t)ii * lo];
+      }
+    }
+  }
+  #pragma omp task depend(inout: sjj[0], wjj[0]) firstprivate(sjj, wjj, ss, ws, j, node, nb)
+  { /* border_factorize -> border_potrf (border_kernel_m.f90:9-19) */
+    int r = k_potrf_u(ss, sjj, ss);
+    if (r) dag_note(res, node, r + (j - 1) * nb);
+    k_trsm_lutn(ss, ws, sjj, ss, sjj + (int64_t)ss * ss, ss);
+    k_syrk_ut(ws, ss, sjj + (int64_t)ss * ss, ss, wjj, ws);
+  }
+  for (int i = j + 1; i <= nbk; i++) { /* border_solve -> border_trsm (:21-30) */
+    int nrow = nd_msize(d, i, node);
+    double *ssp = f_sup(f, node, i, j), *sw = f_work(f, node, i, j);
+    #pragma omp task depend(in: sjj[0]) depend(inout: ssp[0], sw[0]) firstprivate(sjj, ssp, sw, nrow, ss, ws)
+    {
+      k_trsm_lutn(ss, nrow, sjj, ss, ssp, ss);
+      k_gemm_tn(ws, nrow, ss, sjj + (int64_t)ss * ss, ss, ssp, ss, sw, ws);
+    }
+  }
+  for (int i = j + 1; i <= nbk; i++) {
+    int nrow = nd_msize(d, i, node);
+    double *si = f_sup(f, node, i, j), *tii = f_matrix(f, node, i, i);
+    #pragma omp task depend(in: si[0]) depend(inout: tii[0]) firstprivate(si, tii, nrow, ss)
+    k_syrk_ut(nrow, ss, si, ss, tii, nrow);                                      /* border_sym_update */
+    for (int k = i + 1; k <= nbk; k++) {                                          /* border_update(i,k,j) */
+      int un = nd_msize(d, i, node), ln = nd_msize(d, k, node);
+      double *sk = f_sup(f, node, k, j), *tki = f_matrix(f, node, k, i);
+      #pragma omp task depend(in: si[0], sk[0]) depend(inout: tki[0]) firstprivate(si, sk, tki, un, ln, ss)
+      k_gemm_tn(un, ln, ss, si, ss, sk, ss, tki, un);
+    }
+  }
+}
+static void dag_extend_add(factors_t *f, const bli_t *b, int cn, int pn) {     /* seq_factorize_m.f90:81-98 as tasks */
+  nd_t *d = f->nd;
+  int nbk = bli_num_block(b, cn);
+  for (int j = 1; j <= nbk; j++) {
+    for (int i = j; i <= nbk; i++) {
+      int gi = bli_gidx(b, cn, i), gj = bli_gidx(b, cn, j);
+      int ci = b->child_num[gi - 1], cj = b->child_num[gj - 1], pi = b->parent_num[gi - 1], pj = b->parent_num[gj - 1];
+      int roff = bli_offset(b, d, cn, i), coff = bli_offset(b, d, cn, j), li, lj;
+      int *il = bli_arr(b, cn, i, &li), *jlc = bli_arr(b, cn, j, &lj);
+      double *from = f_work(f, cn, ci, cj), *to = f_matrix(f, pn, pi, pj);
+      int ldp = nd_msize(d, pj, pn), ldc = nd_wsize(d, cj, cn);
+      if (i == j) {
+        #pragma omp task depend(in: from[0]) depend(mutexinoutset: to[0]) firstprivate(from, to, il, li, coff, ldp, ldc)
+        { /* extend_add_diag -> extend_add_tri (extend_add_kernel_m.f90:20-33) */
+          for (int a = 1; a <= li; a++) for (int c = 1; c <= a; c++)
+            to[(il[c - 1] - 1) + (int64_t)(il[a - 1] - 1) * ldp] += from[(coff + c - 1) + (int64_t)(coff + a - 1) * ldc];
+        }
+      } else {
+        #pragma omp task depend(in: from[0]) depend(mutexinoutset: to[0]) firstprivate(from, to, il, li, jlc, lj, roff, coff, ldp, ldc)
+        { /* extend_add_ndiag -> extend_add_rect (:6-18) */
+          for (int a = 1; a <= li; a++) for (int c = 1; c <= lj; c++)
+            to[(jlc[c - 1] - 1) + (int64_t)(il[a - 1] - 1) * ldp] += from[(coff + c - 1) + (int64_t)(roff + a - 1) * ldc];
+        }
+      }
+    }
+  }
+}
+EXPORT int orc_factorize_dag(orc_t *h, const double *a, int nthreads) {
+  factors_alloc(&h->fac);
+  double *vals = xmalloc(sizeof(double) * (h->nnz ? h->nnz : 1));
+  for (int k = 0; k < h->nnz; k++) vals[k] = a[h->ccs_perm[k] - 1];              /* permutate */
+  factors_t *f = &h->fac;
+  nd_t *d = f->nd;
+  int nn = h->num_node, nt = nthreads > 0 ? nthreads : 1;
+  #pragma omp parallel for num_threads(nt) schedule(dynamic, 16)
+  for (int node = 1; node <= nn; node++) {                                      /* set_zero, per supernode */
+    int nbk = nd_num_matrix_block(d, node);
+    for (int j = 1; j <= nbk; j++) {
+      int ncol = nd_msize(d, j, node);
+      double *t = f_matrix(f, node, j, j);
+      for (int c = 0; c < ncol; c++) for (int r = 0; r <= c; r++) t[r + (int64_t)c * ncol] = 0.0;
+      for (int i = j + 1; i <= nbk; i++) memset(f_matrix(f, node, i, j), 0, sizeof(double) * (size_t)ncol * nd_msize(d, i, node));
+    }
+  }
+  const int *sets = h->node_sets; const jag_t *si = &h->supernodal_index; int nb = d->nb;
+  #pragma omp parallel for num_threads(nt) schedule(dynamic, 16)
+  for (int node = 1; node <= nn; node++) {                                      /* set_coefficient, per supernode */
+    for (int j = sets[node - 1]; j <= sets[node] - 1; j++) {
+      int *rows = ja(si, j); const double *v = vals + (si->ptr[j - 1] - 1);
+      int col = j - sets[node - 1] + 1, bc = div_ceiling(col, nb), bj = mod2(col, nb);
+      for (int i = 0; i < jl(si, j); i++) {
+        int br = div_ceiling(rows[i], nb), bi = mod2(rows[i], nb);
+        double *blk = f_matrix(f, node, br, bc);
+        blk[(bj - 1) + (int64_t)(bi - 1) * nd_msize(d, bc, node)] = v[i];
+      }
+    }
+  }
+  free(vals);
+  int *res = xcalloc(nn, sizeof(int));
+  #pragma omp parallel num_threads(nt)
+  #pragma omp single
+  {
+    for (int node = 1; node <= nn; node++) {                                    /* submission in postorder */
+      dag_supernode(f, node, res);
+      if (nd_exist_border(d, node)) dag_border(f, node, res);
+      if (h->parent[node - 1]) dag_extend_add(f, &h->bli, node, h->parent[node - 1]);
+    }
+  }
+  h->info = 0;
+  for (int node = 1; node <= nn; node++) if (res[node - 1] && !h->info) h->info = h->node_sets[node - 1] - 1 + res[node - 1];
+  free(res);
+  return h->info;
+}
+
+static void dag_supernode(factors_t *f, int node, int *res) {                 /* seq_factorize_m.f90:31-52 as tasks */
+  nd_t *d = f->nd; int nbk = nd_num_matrix_block(d, node), nb = d->nb;
+  for (int j = 1; j <= nd_work_start(d, node) - 1; j++) {
+    int n = nd_msize(d, j, node);
+    double *tjj = f_matrix(f, node, j, j);
+    #pragma omp task depend(inout: tjj[0]) firstprivate(n, tjj, j, node, nb)
+    {
+      int r = k_potrf_u(n, tjj, n);
+      if (r) dag_note(res, node, r + (j - 1) * nb);
+    }
+    for (int i = j + 1; i <= nbk; i++) {
+      int m = nd_msize(d, i, node);
+      double *tij = f_matrix(f, node, i, j);
+      #pragma omp task depend(in: tjj[0]) depend(inout: tij[0]) firstprivate(n, m, tjj, tij)
+      k_trsm_lutn(n, m, tjj, n, tij, n);
+    }
+    for (int i = j + 1; i <= nbk; i++) {
+      int m = nd_msize(d, i, node);
+      double *tij = f_matrix(f, node, i, j), *tii = f_matrix(f, node, i, i);
+      #pragma omp task depend(in: tij[0]) depend(inout: tii[0]) firstprivate(n, m, tij, tii)
+      k_syrk_ut(m, n, tij, n, tii, m);
+      for (int k = i + 1; k <= nbk; k++) {
+        int un = nd_msize(d, i, node), ln = nd_msize(d, k, node);
+        double *tkj = f_matrix(f, node, k, j), *tki = f_matrix(f, node, k, i);
+        #pragma omp task depend(in: tij[0], tkj[0]) depend(inout: tki[0]) firstprivate(un, ln, tij, tkj, tki)
+        k_gemm_tn(un, ln, un, tij, un, tkj, un, tki, un);
+      }
+    }
+  }
+}
+

@@ -56,6 +56,8 @@ def lib():
     L.orc_factorize.argtypes = [vp, F64P]
     L.orc_factorize_parallel.restype = C.c_int
     L.orc_factorize_parallel.argtypes = [vp, F64P, C.c_int]
+    L.orc_factorize_dag.restype = C.c_int
+    L.orc_factorize_dag.argtypes = [vp, F64P, C.c_int]
     L.orc_solve.argtypes = [vp, F64P]
     L.orc_sweep.argtypes = [vp, F64P, C.c_int]
     L.orc_solve_many.argtypes = [vp, F64P, C.c_int, C.c_int64, C.c_int]
@@ -225,9 +227,15 @@ class Oracle:
         lib().orc_set_tile(self._h, node, i, j, f64(vals))
 
     # -- numeric --------------------------------------------------------------
-    def factorize(self, a, nthreads: int = 0) -> int:
+    def factorize(self, a, nthreads: int = 0, schedule: str = "tree") -> int:
+        """Numeric factorization.  nthreads <= 1: the sequential loop
+        (seq_factorize); otherwise schedule "tree" runs the supernodes of one
+        tree level in parallel, "dag" the reference's StarPU task DAG as
+        OpenMP tasks over tiles (starpu_factorize)."""
         a = f64(a)
         if nthreads and nthreads > 1:
+            if schedule == "dag":
+                return lib().orc_factorize_dag(self._h, a, int(nthreads))
             return lib().orc_factorize_parallel(self._h, a, int(nthreads))
         return lib().orc_factorize(self._h, a)
 

@@ -47,3 +47,28 @@ def test_hppllt_fixture(name):
     assert np.linalg.norm(r) / np.linalg.norm(x) <= R.HPPLLT_TEST_TOL
     anorm = np.abs(val).max() * 10
     assert np.abs(r).max() / (anorm * np.abs(x).max() + np.abs(b).max()) < 1e-14
+
+
+@pytest.mark.parametrize("nb", [7, 32, 128])
+def test_task_dag_factorization_matches_sequential(nb):
+    """The CPU baseline's task-DAG schedule (the StarPU path's tile tasks as
+    OpenMP tasks) against the sequential loop, on fronts with and without
+    border tile columns: the same factor to rounding (the extend-adds into one
+    parent tile commute, so their order may differ) and the same pivot info
+    for a matrix that is not positive definite."""
+    from mfdag import problems as P
+    O.use_system_blas(True)
+    p = P.laplace3d(14)
+    xs = []
+    for sched in ("seq", "dag"):
+        o = O.Oracle.analyze(p.n, p.col, p.row, nb=nb, max_zero=200, order_perm=p.order)
+        assert (o.factorize(p.val) if sched == "seq" else o.factorize(p.val, nthreads=6, schedule="dag")) == 0
+        xs.append(o.solve(p.rhs))
+    assert np.abs(xs[0] - xs[1]).max() <= 1e-13 * np.abs(xs[0]).max()
+    bad = p.val.copy()
+    bad[p.col[300] - 1] = -1.0
+    infos = []
+    for sched in ("seq", "dag"):
+        o = O.Oracle.analyze(p.n, p.col, p.row, nb=nb, max_zero=200, order_perm=p.order)
+        infos.append(o.factorize(bad) if sched == "seq" else o.factorize(bad, nthreads=6, schedule="dag"))
+    assert infos[0] > 0 and infos[0] == infos[1]

@@ -147,9 +147,15 @@ def test_toy_local_and_supernodal_index():               # the toy's own index d
 
 
 @pytest.mark.parametrize("nb,expect", [(2, R.TOY_FACTOR_NB2), (3, R.TOY_FACTOR_NB3)])
-def test_seq_factorize_toy(nb, expect):                  # seq_factorize_test.f90:23-100
+@pytest.mark.parametrize("schedule", ["seq", "dag"])
+def test_seq_factorize_toy(nb, expect, schedule):       # seq_factorize_test.f90:23-100
+    """The integer-exact factor of the reference's toy fixture, from the
+    sequential loop (seq_factorize) and from the task DAG of the StarPU path
+    (starpu_factorize_m.f90, task_test/starpu_factorize_test.f90:103-148
+    checks the same values through StarPU) on 4 threads."""
     o, *_ = _toy(nb)
-    assert o.factorize(np.array(R.TOY_VALUES, dtype=np.float64)) == 0
+    vals = np.array(R.TOY_VALUES, dtype=np.float64)
+    assert (o.factorize(vals) if schedule == "seq" else o.factorize(vals, nthreads=4, schedule="dag")) == 0
     for e in expect:
         kind, node, i, j, vals = e[:5]
         t = o.tile(node, i, j, buffer=1)

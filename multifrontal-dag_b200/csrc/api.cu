@@ -211,6 +211,10 @@ struct mfd_handle {
   double setup_s[4] = {0, 0, 0, 0};                 // analysis, plan, device index maps + exports, CSR + storage
   cudaGraphExec_t g_factor = nullptr;
   std::map<int, cudaGraphExec_t> g_solve;
+  std::map<int, cudaGraphExec_t> g_ir;              // FP32 + FP64 refinement, whole loop per RHS count
+  cudaStream_t bst = nullptr;                       // captures the refinement loop's body
+  DBuf<int32_t> d_ir_i;                             // refinement state (launch_ir_init / launch_ir_check)
+  DBuf<double> d_ir_d, d_ir_prev;
 
   // per-kernel-class profiling (graphs off while enabled)
   bool profiling = false;
@@ -224,6 +228,8 @@ struct mfd_handle {
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     if (g_factor) cudaGraphExecDestroy(g_factor);
     for (auto& kv : g_solve) cudaGraphExecDestroy(kv.second);
+    for (auto& kv : g_ir) cudaGraphExecDestroy(kv.second);
+    if (bst) cudaStreamDestroy(bst);
     for (void* p : {d_panel, d_upool, d_diag, d_X, d_V, d_S})
       if (p) cudaFree(p);
     if (ev0) cudaEventDestroy(ev0);
@@ -675,6 +681,8 @@ int ensure_rhs(mfd_handle* h, int nrhs) {
   if (nrhs <= h->nrhs_cap) return MFD_OK;
   for (auto& kv : h->g_solve) cudaGraphExecDestroy(kv.second);
   h->g_solve.clear();
+  for (auto& kv : h->g_ir) cudaGraphExecDestroy(kv.second);
+  h->g_ir.clear();
   size_t esz = h->fp32 ? sizeof(float) : sizeof(double);
   for (void** p : {&h->d_X, &h->d_V, &h->d_S})
     if (*p) { cudaFree(*p); *p = nullptr; }
@@ -687,6 +695,11 @@ int ensure_rhs(mfd_handle* h, int nrhs) {
   CK(h->d_r.alloc((size_t)h->n_total * nrhs));
   CK(h->d_cnorms.alloc((size_t)8 * nrhs));
   if (h->fp32 && nrhs >= kResMulti) CK(h->d_xt.alloc((size_t)h->n_total * nrhs));
+  if (h->fp32) {
+    CK(h->d_ir_i.alloc(2));
+    CK(h->d_ir_d.alloc(2));
+    CK(h->d_ir_prev.alloc(nrhs));
+  }
   h->nrhs_cap = nrhs;
   return MFD_OK;
 }
@@ -1114,6 +1127,94 @@ int residual_report(mfd_handle* h, const double* xp, const double* bp, mfd_repor
   return MFD_OK;
 }
 
+// One refinement sweep on `st`: x_32 = r in FP32, the FP32 solve, x += x_32
+// in FP64, r = b - A x and the per-column norms (launch_norms layout) in FP64.
+// graph_solve: the FP32 solve as its cached graph (host-driven loop), else its
+// launches directly (inside the refinement graph's body).
+int ir_sweep(mfd_handle* h, int nrhs, cudaStream_t st, bool graph_solve) {
+  const int64_t n = h->n_total;
+  launch_to_t<float>(h->d_r.p, static_cast<float*>(h->d_X), n * nrhs, st);
+  if (graph_solve) {
+    int rc = solve_core<float>(h, nrhs);
+    if (rc) return rc;
+  } else {
+    h->launches_solve = enqueue_solve_core<float>(h, nrhs, st);
+  }
+  launch_axpy_from_t<float>(static_cast<float*>(h->d_X), h->d_xp.p, n * nrhs, st);
+  if (nrhs >= kResMulti) {               // A read once for all columns
+    launch_residual_multi(h->d_csr_ptr.p, h->d_csr_col.p, h->d_csr_val.p, h->d_xp.p, h->d_xt.p, h->d_bp.p,
+                          h->d_r.p, n, nrhs, h->d_cnorms.p, st);
+  } else {
+    for (int r = 0; r < nrhs; ++r) {
+      const int64_t o = (int64_t)r * n;
+      launch_residual(h->d_csr_ptr.p, h->d_csr_col.p, h->d_csr_val.p, h->d_xp.p + o, h->d_bp.p + o, h->d_r.p + o, n,
+                      st);
+      launch_norms(h->d_r.p + o, h->d_xp.p + o, h->d_bp.p + o, n, h->d_cnorms.p + 8 * r, st);
+    }
+  }
+  CK(cudaGetLastError());
+  return MFD_OK;
+}
+
+// The whole refinement of one solve as a graph (built once per RHS count):
+// permutation, x = 0, r = b, state reset; a WHILE node around the sweep, whose
+// body ends with the device convergence test setting the node's condition;
+// the inverse permutation.  Launched on h->st.
+int ir_graph(mfd_handle* h, int nrhs) {
+  cudaGraphExec_t& exec = h->g_ir[nrhs];
+  if (!exec) {
+    const int64_t n = h->n_total;
+    const int maxit = h->opt.ir_max_iter > 0 ? h->opt.ir_max_iter : 20;
+    cudaStream_t st = h->st;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    launch_permute_in<double>(h->d_b.p, n, h->d_perm.p, h->d_bp.p, n, n, nrhs, st);
+    cudaMemsetAsync(h->d_xp.p, 0, sizeof(double) * n * nrhs, st);
+    cudaMemcpyAsync(h->d_r.p, h->d_bp.p, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, st);
+    launch_ir_init(h->d_ir_i.p, h->d_ir_d.p, h->d_ir_prev.p, nrhs, st);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+    cudaGraphConditionalHandle cond = 0;
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode = nullptr;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&wnode, g, deps, ndeps, &cp);
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(st, &wnode, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess) {
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(h->bst, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        int rc = ir_sweep(h, nrhs, h->bst, /*graph_solve=*/false);
+        launch_ir_check(h->d_cnorms.p, h->d_norms.p + 7, nrhs, h->opt.ir_tol, maxit, h->d_ir_prev.p, h->d_ir_i.p,
+                        h->d_ir_d.p, cond, h->bst);
+        cudaGraph_t got = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(h->bst, &got);
+        if (rc != MFD_OK) e = cudaErrorUnknown;
+        else if (e2 != cudaSuccess) e = e2;
+      }
+    }
+    launch_permute_out<double>(h->d_xp.p, n, h->d_perm.p, h->d_b.p, n, n, nrhs, st);
+    cudaGraph_t outer = nullptr;
+    cudaError_t e3 = cudaStreamEndCapture(st, &outer);
+    if (e == cudaSuccess) e = e3;
+    if (e == cudaSuccess) e = cudaGraphInstantiateWithFlags(&exec, outer, cudaGraphInstantiateFlagUseNodePriority);
+    if (outer) cudaGraphDestroy(outer);
+    if (e != cudaSuccess) {
+      exec = nullptr;
+      h->g_ir.erase(nrhs);
+      return fail(MFD_E_CUDA, std::string("refinement graph: ") + cudaGetErrorString(e));
+    }
+  }
+  CK(cudaGraphLaunch(exec, h->st));
+  return MFD_OK;
+}
+
 int do_solve(mfd_handle* h, double* b, int nrhs, int64_t ldb, mfd_report* rep) {
   if (!h->factored) return fail(MFD_E_STATE, "solve before a successful factorize");
   if (!b || nrhs < 1 || ldb < h->n_total) return fail(MFD_E_ARG, "bad right-hand side");
@@ -1144,10 +1245,29 @@ int do_solve(mfd_handle* h, double* b, int nrhs, int64_t ldb, mfd_report* rep) {
       if (rc) return rc;
     }
     launch_permute_out<double>(static_cast<double*>(h->d_X), n, h->d_perm.p, h->d_b.p, n, n, nrhs, st);
+  } else if (h->opt.use_graph && !h->profiling) {
+    // FP32 factor + FP64 iterative refinement as one graph per right-hand-side
+    // count: the sweeps run in a WHILE node whose last kernel applies the
+    // convergence test on the device, so the host waits once per solve
+    rc = ir_graph(h, nrhs);
+    if (rc) return rc;
+    int32_t si[2];
+    double sd[2];
+    CK(cudaMemcpyAsync(si, h->d_ir_i.p, sizeof(si), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(sd, h->d_ir_d.p, sizeof(sd), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(h->ev1, st));
+    CK(cudaStreamSynchronize(st));
+    iters = si[0];
+    bwd = sd[0];
+    if (rep) {
+      rep->backward_error = bwd;
+      rep->residual_ref = sd[1];
+    }
+    if (!(bwd <= h->opt.ir_tol)) rc = MFD_E_NOCONV;
   } else {
-    // FP32 factor + FP64 iterative refinement, all right-hand sides together:
-    // one FP32 multi-RHS solve per sweep, FP64 residual and update per column,
-    // until every column's backward error is below the tolerance (or stagnates)
+    // FP32 factor + FP64 iterative refinement, all right-hand sides together,
+    // the convergence test on the host after every sweep (schedule without
+    // graphs, and the per-kernel profiling runs)
     launch_permute_in<double>(h->d_b.p, n, h->d_perm.p, h->d_bp.p, n, n, nrhs, st);
     CK(cudaMemsetAsync(h->d_xp.p, 0, sizeof(double) * n * nrhs, st));
     CK(cudaMemcpyAsync(h->d_r.p, h->d_bp.p, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, st));
@@ -1156,21 +1276,8 @@ int do_solve(mfd_handle* h, double* b, int nrhs, int64_t ldb, mfd_report* rep) {
     double worst_ref = 0;
     int it = 0;
     for (; it < maxit; ++it) {
-      launch_to_t<float>(h->d_r.p, static_cast<float*>(h->d_X), n * nrhs, st);
-      rc = solve_core<float>(h, nrhs);
+      rc = ir_sweep(h, nrhs, st, /*graph_solve=*/true);
       if (rc) return rc;
-      launch_axpy_from_t<float>(static_cast<float*>(h->d_X), h->d_xp.p, n * nrhs, st);
-      if (nrhs >= kResMulti) {               // A read once for all columns
-        launch_residual_multi(h->d_csr_ptr.p, h->d_csr_col.p, h->d_csr_val.p, h->d_xp.p, h->d_xt.p, h->d_bp.p,
-                              h->d_r.p, n, nrhs, h->d_cnorms.p, st);
-      } else {
-        for (int r = 0; r < nrhs; ++r) {
-          const int64_t o = (int64_t)r * n;
-          launch_residual(h->d_csr_ptr.p, h->d_csr_col.p, h->d_csr_val.p, h->d_xp.p + o, h->d_bp.p + o,
-                          h->d_r.p + o, n, st);
-          launch_norms(h->d_r.p + o, h->d_xp.p + o, h->d_bp.p + o, n, h->d_cnorms.p + 8 * r, st);
-        }
-      }
       CK(cudaMemcpyAsync(nv.data(), h->d_cnorms.p, sizeof(double) * 8 * nrhs, cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
       bool all_ok = true, all_stalled = it > 2;
@@ -1238,6 +1345,7 @@ int create_common(mfd_handle** out, std::vector<Symbolic>&& syms, const mfd_opti
   CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   CK(cudaStreamCreateWithPriority(&h->st, cudaStreamNonBlocking, prio_hi));
   CK(cudaStreamCreateWithPriority(&h->st2, cudaStreamNonBlocking, prio_lo));
+  CK(cudaStreamCreateWithPriority(&h->bst, cudaStreamNonBlocking, prio_hi));
   CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
   for (int k = 0; k < mfd_handle::kMaxDefer; ++k) CK(cudaEventCreateWithFlags(&h->ev_part[k], cudaEventDisableTiming));

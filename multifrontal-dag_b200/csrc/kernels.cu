@@ -2780,6 +2780,50 @@ void launch_axpy_from_t(const T* d, double* x, int64_t n, cudaStream_t st) {
 void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
   if (n > 0) k_fill_int<<<grid_1d(n), 256, 0, st>>>(p, v, n);
 }
+__global__ void k_ir_init(int32_t* st_i, double* st_d, double* prev, int nrhs) {
+  for (int c = threadIdx.x; c < nrhs; c += blockDim.x) prev[c] = 1e300;
+  if (threadIdx.x == 0) {
+    st_i[0] = 0;
+    st_i[1] = 1;
+    st_d[0] = st_d[1] = 0.0;
+  }
+}
+void launch_ir_init(int32_t* st_i, double* st_d, double* prev, int nrhs, cudaStream_t st) {
+  k_ir_init<<<1, 128, 0, st>>>(st_i, st_d, prev, nrhs);
+}
+// one thread: the per-column test in column order, as the host loop does it
+__global__ void k_ir_check(const double* norms, const double* anorm, int nrhs, double tol, int maxit, double* prev,
+                           int32_t* st_i, double* st_d, cudaGraphConditionalHandle cond) {
+  if (threadIdx.x != 0) return;
+  const int it = st_i[0];                 // 0-based index of the sweep just done
+  bool all_ok = true, all_stalled = it > 2;
+  double worst = 0.0, worst_ref = 0.0;
+  for (int c = 0; c < nrhs; ++c) {
+    const double* v = norms + 8 * c;
+    const double denom = anorm[0] * v[1] + v[2];
+    const double cur = denom > 0 ? v[0] / denom : v[0];
+    if (cur > tol) {
+      all_ok = false;
+      if (cur <= 0.9 * prev[c]) all_stalled = false;
+    }
+    if (cur >= worst) {
+      worst = cur;
+      worst_ref = v[4] > 0 ? sqrt(v[3]) / sqrt(v[4]) : sqrt(v[3]);
+    }
+    prev[c] = cur;
+  }
+  st_i[0] = it + 1;
+  st_d[0] = worst;
+  st_d[1] = worst_ref;
+  const bool more = !(all_ok || all_stalled) && it + 1 < maxit;
+  st_i[1] = more ? 1 : 0;
+  cudaGraphSetConditional(cond, more ? 1u : 0u);
+}
+void launch_ir_check(const double* norms, const double* anorm, int nrhs, double tol, int maxit, double* prev,
+                     int32_t* st_i, double* st_d, cudaGraphConditionalHandle cond, cudaStream_t st) {
+  k_ir_check<<<1, 32, 0, st>>>(norms, anorm, nrhs, tol, maxit, prev, st_i, st_d, cond);
+}
+
 __global__ void k_remap_int(const int32_t* map, int32_t* a, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     a[i] = map[a[i]];

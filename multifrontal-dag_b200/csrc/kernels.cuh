@@ -211,4 +211,17 @@ void launch_fill_int(int32_t* p, int32_t v, int64_t n, cudaStream_t st);
 // a[i] = map[a[i]] for i < n
 void launch_remap_int(const int32_t* map, int32_t* a, int64_t n, cudaStream_t st);
 
+// Device-side refinement control (the FP32 + FP64 refinement loop as a graph
+// WHILE node).  State: st_i[0] sweeps done, st_i[1] 1 while refining;
+// st_d[0] the worst column's backward error, st_d[1] its residual_ref; prev[c]
+// each column's previous backward error.  ir_init resets it; ir_check, after a
+// sweep's residual norms (out + 8 c as launch_norms / launch_residual_multi
+// write them) and with anorm = max_i sum_j |a_ij|, applies the host loop's test
+// -- stop when every column is below tol, or from the fourth sweep on when
+// every column above tol has gained less than 10%, or after maxit sweeps --
+// and sets the WHILE node's condition.
+void launch_ir_init(int32_t* st_i, double* st_d, double* prev, int nrhs, cudaStream_t st);
+void launch_ir_check(const double* norms, const double* anorm, int nrhs, double tol, int maxit, double* prev,
+                     int32_t* st_i, double* st_d, cudaGraphConditionalHandle cond, cudaStream_t st);
+
 }  // namespace mfd

@@ -373,6 +373,28 @@ def test_without_graphs_matches():
     assert np.array_equal(x0, x1)
 
 
+@pytest.mark.parametrize("nrhs", [1, 10])
+def test_refinement_graph_matches_host_loop(nrhs):
+    """FP32 + FP64 refinement as one graph with a device-side WHILE condition
+    (the default) and as the host-driven loop (graphs off): the same sweeps
+    in the same order stop at the same sweep with bit-identical solutions."""
+    p = P.laplace3d(16)
+    rng = np.random.default_rng(3)
+    B = np.asfortranarray(rng.uniform(-1, 1, (p.n, nrhs)))
+    out = []
+    for ug in (1, 0):
+        s = gpu_for(p, precision=H.MFD_PREC_FP32_IR, small_front_max=48, use_graph=ug)
+        X = B.copy(order="F")
+        rep, rc = s.solve(X if nrhs > 1 else X[:, 0])
+        assert rc == 0 and rep.converged == 1 and rep.backward_error <= 1e-12
+        out.append((X, rep.iterations, rep.backward_error))
+        X2 = B.copy(order="F")                          # a second solve on the same handle
+        s.solve(X2 if nrhs > 1 else X2[:, 0])
+        assert np.array_equal(X, X2)
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
+
+
 def test_not_positive_definite_reports_pivot():
     p = P.laplace2d(12)
     val = p.val.copy()

@@ -173,13 +173,14 @@ struct mfd_handle {
   std::vector<int32_t> h_lists;
   std::vector<int> small_bins;
   int64_t panel_elems = 0, upool_elems = 0, v_elems = 0, s_elems = 0, dinv_elems = 0;
+  int64_t q_elems = 0;                              // packed FP32 update operands of one step parity
   int32_t max_large_count = 0, max_nf = 0;
   int64_t cost = 0, nonzero = 0;
 
   // device tables
   DBuf<int32_t> d_nc, d_nr, d_first, d_parent, d_child_ptr, d_child, d_lrow_off, d_lrow, d_local, d_a_beg, d_a_src,
       d_a_pos, d_sidx, d_lists, d_perm, d_info, d_cnt;
-  DBuf<int64_t> d_panel_off, d_u_off, d_v_off, d_s_off, d_d_off;
+  DBuf<int64_t> d_panel_off, d_u_off, d_v_off, d_s_off, d_d_off, d_q_off;
   DevFronts F{};
 
   // CSR of the permuted full matrix (residuals)
@@ -192,6 +193,7 @@ struct mfd_handle {
   void* d_panel = nullptr;
   void* d_upool = nullptr;
   void* d_diag = nullptr;
+  float* d_q = nullptr;                             // FP32: packed update operands, two step parities
   DBuf<double> d_a, d_b, d_xp, d_bp, d_r, d_norms, d_cnorms, d_xt;
   void* d_X = nullptr;   // T, n_total x nrhs
   void* d_V = nullptr;   // T
@@ -230,7 +232,7 @@ struct mfd_handle {
     for (auto& kv : g_solve) cudaGraphExecDestroy(kv.second);
     for (auto& kv : g_ir) cudaGraphExecDestroy(kv.second);
     if (bst) cudaStreamDestroy(bst);
-    for (void* p : {d_panel, d_upool, d_diag, d_X, d_V, d_S})
+    for (void* p : {d_panel, d_upool, d_diag, d_X, d_V, d_S, static_cast<void*>(d_q)})
       if (p) cudaFree(p);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -333,6 +335,7 @@ int build_plan(mfd_handle* h) {
   // panel offsets, solve vector offsets, large-front solve scratch
   const int sfm = small_front_max(h);
   h->panel_elems = h->v_elems = h->s_elems = h->dinv_elems = 0;
+  h->q_elems = 0;
   h->max_nf = 0;
   for (int32_t g = 0; g < nfr; ++g) {
     HostFront& fr = h->fronts[g];
@@ -426,6 +429,18 @@ int build_plan(mfd_handle* h) {
     L.large.param = max_entries;
     L.large.param2 = max_nc;
     L.large_zero_elems = max_elems;
+    // packed operands of the FP32 tensor-core update: the level's large fronts side by side,
+    // each with the 128-row blocks of its largest step (step 0); reused level after level
+    {
+      int64_t q = 0;
+      for (int32_t g : large) {
+        HostFront& fr = h->fronts[g];
+        const int64_t nrem = (int64_t)fr.nc + fr.nr - std::min(kFactB, fr.nc);
+        fr.q_off = q;
+        q += (nrem + kFactB - 1) / kFactB * kPackedBlockElems;
+      }
+      h->q_elems = std::max(h->q_elems, q);
+    }
     // extend-add by child rank
     for (int rank = 0;; ++rank) {
       std::vector<int32_t> kids;
@@ -475,11 +490,12 @@ int upload_plan(mfd_handle* h) {
   cudaStream_t st = h->st;
   const int32_t nfr = h->num_front;
   std::vector<int32_t> nc(nfr), nr(nfr), first(nfr), parent(nfr);
-  std::vector<int64_t> poff(nfr), uoff(nfr), voff(nfr), soff(nfr), doff(nfr);
+  std::vector<int64_t> poff(nfr), uoff(nfr), voff(nfr), soff(nfr), doff(nfr), qoff(nfr);
   for (int32_t g = 0; g < nfr; ++g) {
     const HostFront& f = h->fronts[g];
     nc[g] = f.nc; nr[g] = f.nr; first[g] = f.first; parent[g] = f.parent;
     poff[g] = f.panel_off; uoff[g] = f.u_off; voff[g] = f.v_off; soff[g] = f.s_off; doff[g] = f.d_off;
+    qoff[g] = f.q_off;
   }
   std::vector<int32_t> lrow_glob;
   lrow_glob.reserve(h->h_lrow_off[nfr]);
@@ -500,6 +516,7 @@ int upload_plan(mfd_handle* h) {
   CK(h->d_v_off.upload(voff, st));
   CK(h->d_s_off.upload(soff, st));
   CK(h->d_d_off.upload(doff, st));
+  CK(h->d_q_off.upload(qoff, st));
   CK(h->d_lists.upload(h->h_lists, st));
   CK(h->d_a_src.alloc(h->nnz_total));
   CK(h->d_a_pos.alloc(h->nnz_total));
@@ -516,6 +533,7 @@ int upload_plan(mfd_handle* h) {
   F.lrow_off = h->d_lrow_off.p; F.lrow = h->d_lrow.p; F.local = h->d_local.p; F.a_beg = h->d_a_beg.p;
   F.a_src = h->d_a_src.p; F.a_pos = h->d_a_pos.p; F.v_off = h->d_v_off.p; F.s_off = h->d_s_off.p;
   F.d_off = h->d_d_off.p;
+  F.q_off = h->d_q_off.p;
 
   // permuted global A structure, value sources, front of every column
   std::vector<int32_t> acol(h->n_total + 1), arow(h->nnz_total), src(h->nnz_total), colf(h->n_total),
@@ -665,9 +683,16 @@ int upload_plan(mfd_handle* h) {
 
   // numeric storage
   size_t esz = h->fp32 ? sizeof(float) : sizeof(double);
-  CK(cudaMalloc(&h->d_panel, std::max<int64_t>(h->panel_elems, 1) * esz));
+  // 32 elements of slack: the FP32 tensor-core update copies column segments
+  // in 16-byte chunks and may read up to 3 elements past the last panel
+  CK(cudaMalloc(&h->d_panel, (std::max<int64_t>(h->panel_elems, 1) + 32) * esz));
   CK(cudaMalloc(&h->d_upool, std::max<int64_t>(h->upool_elems, 1) * esz));
   CK(cudaMalloc(&h->d_diag, (size_t)std::max<int64_t>(h->dinv_elems, 1) * esz));
+  if (h->fp32 && h->q_elems > 0) {
+    CK(cudaMalloc(&h->d_q, (size_t)(2 * h->q_elems) * sizeof(float)));
+    // rows past a front's last row are never written and only reach discarded outputs; zero keeps them finite
+    CK(cudaMemsetAsync(h->d_q, 0, (size_t)(2 * h->q_elems) * sizeof(float), h->st));
+  }
   // the inverted diagonal blocks are written on their lower w x w part only: the rest stays zero
   CK(cudaMemsetAsync(h->d_diag, 0, (size_t)std::max<int64_t>(h->dinv_elems, 1) * esz, h->st));
   h->a_len = h->nnz_total;
@@ -850,6 +875,10 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
     // SMs the side-stream update could use), so the default leaves it off.
     const bool pdl = h->opt.reserved[2] == 1 && !h->profiling;
     const int D = h->defer;
+    // FP32 tensor-core update without deferral: the TRSM also writes the step's rows as
+    // packed TF32 hi / lo operands (two buffers by step parity: with D = 1 the bulk update
+    // of step s is complete before the TRSM of step s + 2 starts) for k_update_tcq
+    const bool tcq = sizeof(T) == 4 && (kind == 0 || kind == 2) && D == 1 && h->d_q != nullptr;
     int pend = -1;                            // step of the latest bulk on st2 not yet fully waited for
     for (size_t s = 0; s < L.steps.size(); ++s) {
       const LaunchList& p = L.steps[s];
@@ -890,7 +919,8 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
              [&] { launch_potrf<T>(F, lists + p.off, p.count, (int)s, panel, diag, h->d_info.p, st, pdl, 0,
                                    h->d_info.p + 3); });
       record(h, st, MFD_K_TRSM, tf, tb, [&] {
-        launch_trsm<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, kind == 1 ? 1 : 0, st, pdl);
+        launch_trsm<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, kind == 1 ? 1 : 0, st, pdl,
+                       tcq ? h->d_q + (s & 1) * h->q_elems : nullptr);
       });
       n += 2;
       auto update = [&](cudaStream_t us, UpdBand band) {
@@ -899,6 +929,12 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
         const bool upd_pdl = pdl && us == st;        // right behind the TRSM on the main stream
         record(h, us, MFD_K_UPDATE, fl, by, [&] {
           if constexpr (sizeof(T) == 4) {
+            if (tcq) {
+              n += launch_update_tcq(F, lists + p.off, p.count, (int)s, p.param2, h->d_q + (s & 1) * h->q_elems,
+                                     reinterpret_cast<float*>(panel), reinterpret_cast<float*>(upool),
+                                     kind == 0 ? 1 : 0, h->d_info.p + 1, us, band, upd_pdl);
+              return;
+            }
             if (kind == 0 || kind == 2) {
               n += launch_update_tc(F, lists + p.off, p.count, (int)s, p.param2, reinterpret_cast<float*>(panel),
                                     reinterpret_cast<float*>(upool), kind == 0 ? 1 : 0, h->d_info.p + 1, us, band,

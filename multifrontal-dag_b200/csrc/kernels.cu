@@ -936,7 +936,8 @@ constexpr size_t trsm2_smem() {
 
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_trsm2(DevFronts F, const int32_t* list, int step, T* panel, const T* linv) {
+__global__ void __launch_bounds__(256) k_trsm2(DevFronts F, const int32_t* list, int step, T* panel, const T* linv,
+                                               float* q) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* As = reinterpret_cast<T*>(smem_raw);            // [k][row]
   T* Bs = As + kFactB * kTr2LdA;                      // [k][n]: Li(n, k)
@@ -1013,6 +1014,22 @@ __global__ void __launch_bounds__(256) k_trsm2(DevFronts F, const int32_t* list,
         const int gi = r0 + ty + 16 * l, n = tx + 16 * m;
         if (gi < nf && n < w) P[gi + (size_t)(c0 + n) * nf] = acc[l][m];
       }
+    if (q != nullptr) {     // the same rows as packed TF32 hi / lo operands of the tensor-core update
+      float* Q = q + F.q_off[f];
+      const int rrel = blockIdx.x * kTr2Rows;                 // first row of the CTA relative to c0 + w
+#pragma unroll
+      for (int l = 0; l < 2; ++l)
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          const int rr = rrel + ty + 16 * l, n = tx + 16 * m;
+          const float v = (r0 + ty + 16 * l < nf && n < w) ? (float)acc[l][m] : 0.0f;
+          uint32_t hb;
+          asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(v));
+          const float hi = __uint_as_float(hb);
+          Q[packed_offset(rr, n, 0)] = hi;
+          Q[packed_offset(rr, n, 1)] = v - hi;
+        }
+    }
   }
 }
 
@@ -2550,6 +2567,7 @@ cudaError_t prepare_kernels() {
   chk(opt_in(k_update_dmma));
   chk(opt_in(k_potrf<double>)); chk(opt_in(k_potrf<float>));
   chk(prepare_update_tc());
+  chk(prepare_update_tcq());
   chk(opt_in(k_update_simt<double>)); chk(opt_in(k_update_simt<float>));
   chk(opt_in(k_update_dmma2));
   return e;
@@ -2621,12 +2639,13 @@ void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, 
 }
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
-                 const T* linv, int kind, cudaStream_t st, bool pdl) {
+                 const T* linv, int kind, cudaStream_t st, bool pdl, float* q) {
   if (count <= 0 || row_blocks <= 0) return;
   (void)kind;
   // row_blocks counts 64-row blocks
   dim3 grid(row_blocks * 2, count);
-  launch_k(k_trsm2<T>, grid, dim3(256), trsm2_smem<T>(), st, pdl, F, list, step, panel, linv);
+  launch_k(k_trsm2<T>, grid, dim3(256), trsm2_smem<T>(), st, pdl, F, list, step, panel, linv,
+           sizeof(T) == 4 ? q : nullptr);
 }
 int update_grid(int T, int tw, UpdBand band) {
   const int c1 = kFactB / tw, jlo = band.blo * c1;
@@ -2842,7 +2861,7 @@ void launch_remap_int(const int32_t* map, int32_t* a, int64_t n, cudaStream_t st
   template void launch_potrf<T>(const DevFronts&, const int32_t*, int, int, T*, T*, int32_t*, cudaStream_t, bool,  \
                                 int, int32_t*);                                                                    \
   template void launch_trsm<T>(const DevFronts&, const int32_t*, int, int, int, T*, const T*, int, cudaStream_t,   \
-                               bool);                                                                              \
+                               bool, float*);                                                                           \
   template int launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t,    \
                                  UpdBand, int, bool);                                                              \
   template void launch_fwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, T*, int,    \

@@ -141,9 +141,11 @@ void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int m
 template <typename T>
 void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
                   cudaStream_t st, bool pdl = false, int info_stride = 0, int32_t* fallbacks = nullptr);
+// q (FP32 only, may be null): also write the solved rows as packed TF32 operands of the
+// tensor-core update (packed_offset below), at q + F.q_off[f].
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
-                 const T* linv, int kind, cudaStream_t st, bool pdl = false);
+                 const T* linv, int kind, cudaStream_t st, bool pdl = false, float* q = nullptr);
 // Trailing update of step `step` over the tile-column band [blo, bhi) (128-column blocks relative to
 // the trailing matrix, bhi < 0: to the end; see select_tile) with updates deferred over groups of
 // `defer` steps (update_k_range).  T128 / T64: the largest front's trailing tiles per side.
@@ -161,6 +163,27 @@ cudaError_t prepare_update_tc();
 int launch_update_tc(const DevFronts& F, const int32_t* list, int count, int step, int T128, float* panel,
                      float* upool, int split, int32_t* err, cudaStream_t st, UpdBand band = {}, int defer = 1,
                      bool pdl = false);
+// Packed operands of the FP32 tensor-core update, written by the TRSM of a panel step: the
+// step's solved rows below the diagonal block, in 128-row blocks rb (rows base + 128 rb ..,
+// base = first row below the block), each as 16 K chunks of 8 columns, each chunk a TF32 hi
+// block then a lo block (x - hi), 1024 floats each in the canonical K-major no-swizzle UMMA
+// layout (8-row x 16-byte core matrices; 16 bytes between the two k-cores, 256 between
+// 8-row groups).  Columns past the block width are zero.  Two buffers, by step parity.
+constexpr int64_t kPackedBlockElems = 16 * 2 * 1024;   // one 128-row block: 16 chunks x (hi, lo)
+#ifdef __CUDACC__
+__host__ __device__ constexpr int64_t packed_block_elems() { return kPackedBlockElems; }
+__device__ __forceinline__ int64_t packed_offset(int row, int k, int hl) {   // row, k: 0-based within the step
+  const int rb = row >> 7, r = row & 127, kc = k >> 3, kk = k & 7;
+  return (int64_t)rb * packed_block_elems() + (int64_t)((kc * 2 + hl) * 1024) + (r >> 3) * 64 + (r & 7) * 4 +
+         (kk >> 2) * 32 + (kk & 3);
+}
+#endif
+// Trailing update of an FP32 step with deferral depth 1 from the packed operands q (this
+// step's parity buffer): warp-specialised tcgen05 pipeline (update_tc.cu).
+cudaError_t prepare_update_tcq();
+int launch_update_tcq(const DevFronts& F, const int32_t* list, int count, int step, int T128, const float* q,
+                      float* panel, float* upool, int split, int32_t* err, cudaStream_t st, UpdBand band = {},
+                      bool pdl = false);
 // grid size of an update launch over a band of the T x T lower tiles of width tw
 int update_grid(int T, int tw, UpdBand band);
 

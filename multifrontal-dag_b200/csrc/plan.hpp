@@ -35,11 +35,12 @@ struct DevFronts {
   const int64_t* s_off;       // scratch offset (large-front solve partial sums)
   const int64_t* d_off;       // offset of f's inverted 128 x 128 diagonal blocks (one per panel step);
                               // null: the inverse of list slot i lives at linv + i * 128 * 128
+  const int64_t* q_off;       // FP32: offset of f's packed update operands (null when unused)
 };
 
 struct HostFront {
   int32_t nc, nr, first, parent, level, sys, node;
-  int64_t panel_off, u_off, v_off, s_off, d_off;
+  int64_t panel_off, u_off, v_off, s_off, d_off, q_off;
 };
 
 struct LaunchList {          // a list of front ids in the device list pool

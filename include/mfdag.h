@@ -58,7 +58,8 @@ typedef struct {
                               [1] = 1 lookahead off, [2] = 1 programmatic launch along the panel
                               chain, [3] = 1 no programmatic launch between solve steps, [4] = 1
                               no side streams per level, [5] = panel steps per deferred trailing
-                              update (1 = none)                                                 */
+                              update (1 = none), [6] = 1 single-RHS large-front solves one launch
+                              per panel step instead of one per level                           */
 } mfd_options;
 
 /* Symbolic data exactly as the reference holds it after hppllt_analyze

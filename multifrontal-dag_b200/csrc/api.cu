@@ -171,6 +171,8 @@ struct mfd_handle {
   std::vector<int32_t> h_child_ptr, h_child, h_lrow_off, h_a_beg;
   std::vector<LevelPlan> levels;
   std::vector<int32_t> h_lists;
+  std::vector<int32_t> h_stasks;                    // fused single-RHS solve tasks, 4 ints each
+  int32_t solve_flags = 0;                          // per front and panel step, one sweep's worth
   std::vector<int> small_bins;
   int64_t panel_elems = 0, upool_elems = 0, v_elems = 0, s_elems = 0, dinv_elems = 0;
   int64_t q_elems = 0;                              // packed FP32 update operands of one step parity
@@ -180,6 +182,9 @@ struct mfd_handle {
   // device tables
   DBuf<int32_t> d_nc, d_nr, d_first, d_parent, d_child_ptr, d_child, d_lrow_off, d_lrow, d_local, d_a_beg, d_a_src,
       d_a_pos, d_sidx, d_lists, d_perm, d_info, d_cnt;
+  // fused solve: the tasks, and [0] expiry flag, [1 + 2 l] / [2 + 2 l] level l's forward /
+  // backward tickets, then forward and backward step flags (zeroed before every solve)
+  DBuf<int32_t> d_stasks, d_ssync;
   DBuf<int64_t> d_panel_off, d_u_off, d_v_off, d_s_off, d_d_off, d_q_off;
   DevFronts F{};
 
@@ -384,6 +389,8 @@ int build_plan(mfd_handle* h) {
   if (h->small_bins.empty() || h->small_bins.back() < sfm) h->small_bins.push_back(sfm);
   h->levels.assign(nlev, LevelPlan{});
   h->h_lists.clear();
+  h->h_stasks.clear();
+  h->solve_flags = 0;
   h->max_large_count = 0;
   std::vector<std::vector<int32_t>> lev_fronts(nlev);
   for (int32_t g = 0; g < nfr; ++g) lev_fronts[h->fronts[g].level].push_back(g);
@@ -481,6 +488,29 @@ int build_plan(mfd_handle* h) {
       ll.param3 = tiles64;
       L.steps.push_back(ll);
     }
+    // single-RHS solve tasks of the level, in dependency order (see launch_large_fused)
+    {
+      auto push_task = [&](int32_t g, int32_t code, int32_t flag) {
+        h->h_stasks.insert(h->h_stasks.end(), {g, code, flag, 0});
+      };
+      std::vector<int32_t> fbase(large.size());
+      for (size_t k = 0; k < large.size(); ++k) {
+        fbase[k] = h->solve_flags;
+        h->solve_flags += (h->fronts[large[k]].nc + kFactB - 1) / kFactB;
+      }
+      L.fwd_tasks.off = (int32_t)(h->h_stasks.size() / 4);
+      for (int s = 0; s < steps; ++s)
+        for (size_t k = 0; k < large.size(); ++k)
+          if (h->fronts[large[k]].nc > s * kFactB) push_task(large[k], s, fbase[k]);
+      for (size_t k = 0; k < large.size(); ++k)
+        for (int j = 0; j * kFactB < h->fronts[large[k]].nr; ++j) push_task(large[k], -1 - j, fbase[k]);
+      L.fwd_tasks.count = (int32_t)(h->h_stasks.size() / 4) - L.fwd_tasks.off;
+      L.bwd_tasks.off = (int32_t)(h->h_stasks.size() / 4);
+      for (int s = steps - 1; s >= 0; --s)
+        for (size_t k = 0; k < large.size(); ++k)
+          if (h->fronts[large[k]].nc > s * kFactB) push_task(large[k], s, fbase[k]);
+      L.bwd_tasks.count = (int32_t)(h->h_stasks.size() / 4) - L.bwd_tasks.off;
+    }
   }
   return MFD_OK;
 }
@@ -518,6 +548,9 @@ int upload_plan(mfd_handle* h) {
   CK(h->d_d_off.upload(doff, st));
   CK(h->d_q_off.upload(qoff, st));
   CK(h->d_lists.upload(h->h_lists, st));
+  if (!h->h_stasks.empty()) CK(h->d_stasks.upload(h->h_stasks, st));
+  CK(h->d_ssync.alloc(1 + 2 * h->levels.size() + 2 * (size_t)h->solve_flags));
+  CK(cudaMemsetAsync(h->d_ssync.p, 0, sizeof(int32_t) * h->d_ssync.n, st));
   CK(h->d_a_src.alloc(h->nnz_total));
   CK(h->d_a_pos.alloc(h->nnz_total));
   CK(h->d_sidx.alloc(h->nnz_total));
@@ -1002,6 +1035,16 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
   // programmatic dependent launch between the large-front solve steps (on
   // unless reserved[3] = 1; the profiling schedule times kernels one by one)
   const bool solve_pdl = h->opt.reserved[3] != 1 && !prof;
+  // one launch per level and sweep for the large fronts' steps (single right-hand side)
+  const bool fused = nrhs == 1 && h->opt.reserved[6] != 1 && !h->h_stasks.empty();
+  const int4* stasks = reinterpret_cast<const int4*>(h->d_stasks.p);
+  int32_t* ssync = h->d_ssync.p;
+  int32_t* fwd_flags = ssync + 1 + 2 * h->levels.size();
+  int32_t* bwd_flags = fwd_flags + h->solve_flags;
+  if (fused) {                              // a kernel, not a memset node: this also runs in the refinement loop's body
+    launch_fill_int(ssync, 0, (int64_t)h->d_ssync.n, st);
+    ++n;
+  }
   // algorithmic work of one sweep over a list: read the panel once, 2 flops per entry per RHS
   auto work = [&](const LaunchList& l, double& fl, double& by) {
     if (!prof) return;
@@ -1036,7 +1079,13 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       work(L.large, fl, by);
       record(h, st, MFD_K_SOLVE_LARGE, fl, by, [&] {
         launch_fwd_large<T>(F, lists + L.large.off, L.large.count, L.large.param2, L.large_max_nf, panel, dinv, X,
-                            ldx, V, h->d_cnt.p, nrhs, st, &n, solve_pdl);
+                            ldx, V, h->d_cnt.p, nrhs, st, &n, solve_pdl, fused);
+        if (fused) {
+          const size_t lv = &L - h->levels.data();
+          launch_large_fused<T>(F, stasks + L.fwd_tasks.off, L.fwd_tasks.count, false, ssync + 1 + 2 * lv, fwd_flags,
+                                ssync, panel, dinv, X, V, st);
+          ++n;
+        }
       });
     }
     if (nside) side_join(h, st, nside);
@@ -1059,7 +1108,13 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
       work(L.large, fl, by);
       record(h, st, MFD_K_SOLVE_LARGE, fl, by, [&] {
         launch_bwd_large<T>(F, lists + L.large.off, L.large.count, L.large.param2, L.large_max_nf, panel, dinv, X,
-                            ldx, V, S, h->d_cnt.p, nrhs, st, &n, solve_pdl);
+                            ldx, V, S, h->d_cnt.p, nrhs, st, &n, solve_pdl, fused);
+        if (fused) {
+          const size_t lv = &L - h->levels.data();
+          launch_large_fused<T>(F, stasks + L.bwd_tasks.off, L.bwd_tasks.count, true, ssync + 2 + 2 * lv, bwd_flags,
+                                ssync, panel, dinv, X, V, st);
+          ++n;
+        }
       });
     }
     if (nside) side_join(h, st, nside);
@@ -1350,7 +1405,10 @@ int do_solve(mfd_handle* h, double* b, int nrhs, int64_t ldb, mfd_report* rep) {
     CK(cudaMemcpy2DAsync(b, sizeof(double) * ldb, h->d_b.p, sizeof(double) * n, sizeof(double) * n, nrhs,
                          dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
   }
+  int32_t expired = 0;                      // a bounded wait of the single-RHS large-front sweeps gave up
+  if (nrhs == 1 && !h->h_stasks.empty()) CK(cudaMemcpyAsync(&expired, h->d_ssync.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  if (expired) return fail(MFD_E_TIMEOUT, "a device wait of the solve timed out");
   float ms = 0;
   cudaEventElapsedTime(&ms, h->ev0, h->ev1);
   collect_profile(h);

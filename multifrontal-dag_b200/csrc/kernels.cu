@@ -1798,7 +1798,7 @@ __device__ void fwd_diag_cta(const DevFronts& F, int f, int step, int slot, cons
 template <typename T>
 __global__ void __launch_bounds__(256) k_fwd_large_gather(DevFronts F, const int32_t* list,
                                                           const T* __restrict__ dinv, T* X, int64_t ldx, T* V,
-                                                          int nrhs) {
+                                                          int nrhs, int diag0) {
   __shared__ T vs[kSolveB * kRhsG];
   __shared__ T hs[kSolveB * kRhsG];
   const int f = list[blockIdx.x];
@@ -1847,7 +1847,7 @@ __global__ void __launch_bounds__(256) k_fwd_large_gather(DevFronts F, const int
       __syncthreads();
     }
   }
-  if (nrhs >= kMrhsMin || gridDim.y > 1) return;   // the GEMM-shaped diagonal kernel follows
+  if (nrhs >= kMrhsMin || gridDim.y > 1 || !diag0) return;   // the GEMM-shaped diagonal kernel (or the fused sweep) follows
   __threadfence_block();
   fwd_diag_cta(F, f, 0, blockIdx.x, dinv, X, ldx, Vbase, nf, nrhs, vs, hs);
 }
@@ -1919,6 +1919,225 @@ __global__ void __launch_bounds__(256) k_fwd_large_rest(DevFronts F, const int32
   __threadfence();
   fwd_diag_cta(F, f, step + 1, blockIdx.y, dinv, X, ldx, Vf, nf, nrhs, vs, hs);
   if (threadIdx.x == 0) cnt[blockIdx.y] = 0;
+}
+
+// ---- single right-hand side: a level's large-front sweep in one launch ----------
+// The sweep is a list of tasks in dependency order: forward, for each panel step
+// s the diagonal-block task (f, s) of every front (y_s = Li (v_s - sum_{t<s}
+// L_st y_t)), then the rest-row tasks (128 rows below the front's columns each,
+// v_rest -= sum_t L_rest,t y_t); backward, for s from the last step down the
+// column-block task (f, s) of every front (x_s = Li^T (v_s - L_below,s^T
+// x_below)).  A CTA takes the next task from a ticket counter, so a task only
+// waits (on the per-front, per-step flags the producing tasks release) for
+// tasks that CTAs already running have taken: the sweep always progresses.
+// Every wait is bounded (~1 s); on expiry the CTA raises `expired` and stops
+// (the solve reports MFD_E_TIMEOUT).  Each task's sums have a fixed order, so
+// the sweep is deterministic.
+constexpr int kFuseRows = 128;                // rows of a forward rest task
+constexpr long long kSolveWaitLimit = 1ll << 31;
+
+__device__ __forceinline__ int ld_acquire_i32(const int32_t* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_i32(int32_t* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// thread 0 waits for *flag != 0 (bounded; gives up at once when another CTA's
+// wait expired); the result is the CTA's
+__device__ __forceinline__ bool cta_wait_flag(const int32_t* flag, int32_t* expired, int* sh_ok) {
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    if (ld_acquire_i32(flag) == 0) {
+      const long long t0 = clock64();
+      while (ld_acquire_i32(flag) == 0) {
+        if (clock64() - t0 > kSolveWaitLimit || ld_acquire_i32(expired) != 0) {
+          ok = 0;
+          atomicExch(expired, 1);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    *sh_ok = ok;
+  }
+  __syncthreads();
+  return *sh_ok != 0;
+}
+
+// forward: thread (row r0 + (t mod 128), half t / 128) sums its half of each
+// step's 128 columns; the step's 64 panel entries are loaded before the wait on
+// y_s (they do not depend on it)
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwd_large_fused(DevFronts F, const int4* __restrict__ tasks, int ntask,
+                                                         int32_t* ticket, int32_t* flags, int32_t* expired,
+                                                         const T* __restrict__ panel, const T* __restrict__ dinv,
+                                                         T* X, T* V) {
+  __shared__ int sh_t, sh_ok;
+  __shared__ T ys[kSolveB];
+  __shared__ T part[kFuseRows];
+  if (threadIdx.x == 0) sh_t = atomicAdd(ticket, 1);
+  __syncthreads();
+  const int t = sh_t;
+  if (t >= ntask) return;
+  const int4 tk = tasks[t];
+  const int f = tk.x, code = tk.y;
+  int32_t* fl = flags + tk.z;
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int r0 = code >= 0 ? code * kSolveB : nc + (-1 - code) * kFuseRows;
+  const int r1 = code >= 0 ? min(nc, r0 + kSolveB) : min(nf, r0 + kFuseRows);
+  const int nsteps = code >= 0 ? code : (nc + kSolveB - 1) / kSolveB;   // steps whose y this task consumes
+  const T* P = panel + F.panel_off[f];
+  T* Vf = V + F.v_off[f];
+  const int tid = threadIdx.x, ri = tid & (kFuseRows - 1), h = tid >> 7;
+  const int i = r0 + ri;
+  const bool valid = i < r1;
+  T acc = T(0);
+  for (int s = 0; s < nsteps; ++s) {
+    const int c0 = s * kSolveB, w = min(kSolveB, nc - c0);
+    T l[64];
+    const T* pc = P + (valid ? i : 0) + (size_t)(c0 + 64 * h) * nf;
+#pragma unroll
+    for (int k = 0; k < 64; ++k) l[k] = (valid && 64 * h + k < w) ? pc[(size_t)k * nf] : T(0);
+    if (!cta_wait_flag(fl + s, expired, &sh_ok)) return;
+    if (tid < kSolveB) ys[tid] = tid < w ? __ldcg(&Vf[c0 + tid]) : T(0);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 64; ++k) acc += l[k] * ys[64 * h + k];
+    __syncthreads();
+  }
+  if (h == 1) part[ri] = acc;
+  __syncthreads();
+  T v = T(0);
+  if (h == 0 && valid) v = Vf[i] - (acc + part[ri]);
+  if (code < 0) {
+    if (h == 0 && valid) Vf[i] = v;
+    return;
+  }
+  if (h == 0) ys[ri] = valid ? v : T(0);
+  __syncthreads();
+  const T* Li = inv_block(F, dinv, f, code, 0);    // zero outside its w x w part
+  T y = T(0);
+#pragma unroll 16
+  for (int k = 0; k < 64; ++k) y += Li[ri + (size_t)(64 * h + k) * kSolveB] * ys[64 * h + k];
+  if (h == 1) part[ri] = y;
+  __syncthreads();
+  if (h == 0 && valid) {
+    const T yy = y + part[ri];
+    Vf[i] = yy;
+    X[F.first[f] + i] = yy;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    st_release_i32(fl + code, 1);
+  }
+}
+
+// backward: warp w takes columns 16 w .. 16 w + 15 of the block, lanes rows;
+// the rows below the block in the update part (their x known from the gather)
+// first, then the later diagonal blocks of the front from the last one down,
+// each after its flag (its panel entries loaded before the wait); a butterfly
+// transpose-reduce leaves column 16 w + (l mod 16)'s sum in lane l.
+template <typename T>
+__device__ __forceinline__ void bwd_rows_acc(const T* P, int nf, int c0, int w, int ra, int rb, const T* Vf, bool cg,
+                                             int wc, int lane, T (&acc)[16]) {
+  for (int rr = ra; rr < rb; rr += 32) {
+    const int r = rr + lane;
+    const bool ok = r < rb;
+    const T xv = ok ? (cg ? __ldcg(&Vf[r]) : Vf[r]) : T(0);
+    const T* pr = P + (ok ? r : ra) + (size_t)(c0 + wc) * nf;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) acc[j] += (ok && wc + j < w ? pr[(size_t)j * nf] : T(0)) * xv;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_bwd_large_fused(DevFronts F, const int4* __restrict__ tasks, int ntask,
+                                                         int32_t* ticket, int32_t* flags, int32_t* expired,
+                                                         const T* __restrict__ panel, const T* __restrict__ dinv,
+                                                         T* X, T* V) {
+  __shared__ int sh_t, sh_ok;
+  __shared__ T ts[kSolveB];
+  if (threadIdx.x == 0) sh_t = atomicAdd(ticket, 1);
+  __syncthreads();
+  const int t = sh_t;
+  if (t >= ntask) return;
+  const int4 tk = tasks[t];
+  const int f = tk.x, s = tk.y;
+  int32_t* fl = flags + tk.z;
+  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int nsteps = (nc + kSolveB - 1) / kSolveB;
+  const int c0 = s * kSolveB, w = min(kSolveB, nc - c0);
+  const T* P = panel + F.panel_off[f];
+  T* Vf = V + F.v_off[f];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wc = 16 * warp;
+  T acc[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) acc[j] = T(0);
+  bwd_rows_acc(P, nf, c0, w, nc, nf, Vf, false, wc, lane, acc);            // update rows: x gathered
+  for (int b = nsteps - 1; b > s; --b) {                                   // later diagonal blocks
+    const int ra = b * kSolveB, rb = min(nc, ra + kSolveB);
+    T l[4][16];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = ra + lane + 32 * q;
+      const T* pr = P + (r < rb ? r : ra) + (size_t)(c0 + wc) * nf;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) l[q][j] = (r < rb && wc + j < w) ? pr[(size_t)j * nf] : T(0);
+    }
+    if (!cta_wait_flag(fl + b, expired, &sh_ok)) return;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = ra + lane + 32 * q;
+      const T xv = r < rb ? __ldcg(&Vf[r]) : T(0);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) acc[j] += l[q][j] * xv;
+    }
+  }
+  // butterfly transpose-reduce: lane l ends with column wc + (l mod 16)'s sum
+#pragma unroll
+  for (int sft = 8; sft >= 1; sft >>= 1) {
+    const bool up = (lane & sft) != 0;
+#pragma unroll
+    for (int j = 0; j < sft; ++j) {
+      const T send = up ? acc[j] : acc[j + sft];
+      const T keep = up ? acc[j + sft] : acc[j];
+      acc[j] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
+    }
+  }
+  acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 16);
+  if (lane < 16) {
+    const int c = wc + lane;
+    ts[c] = c < w ? Vf[c0 + c] - acc[0] : T(0);
+  }
+  __syncthreads();
+  // x = Li^T t: column i of Li against t, lanes over k (coalesced), 16 columns per warp
+  const T* Li = inv_block(F, dinv, f, s, 0);
+  T tv[kSolveB / 32];
+#pragma unroll
+  for (int q = 0; q < kSolveB / 32; ++q) tv[q] = ts[lane + 32 * q];
+  const int first = F.first[f];
+#pragma unroll 4
+  for (int cc = 0; cc < 16; ++cc) {
+    const int i = wc + cc;
+    const T* lcol = Li + (size_t)i * kSolveB + lane;
+    T sum = T(0);
+#pragma unroll
+    for (int q = 0; q < kSolveB / 32; ++q) sum += lcol[32 * q] * tv[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0 && i < w) {
+      Vf[c0 + i] = sum;
+      X[first + c0 + i] = sum;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release_i32(fl + s, 1);
+  }
 }
 
 template <typename T>
@@ -2710,9 +2929,14 @@ void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
                       const T* dinv, T* X, int64_t ldx, T* V, int32_t* cnt, int nrhs, cudaStream_t st,
-                      int64_t* launches, bool pdl) {
+                      int64_t* launches, bool pdl, bool fused) {
   if (count <= 0) return;
-  k_fwd_large_gather<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, 0, st>>>(F, list, dinv, X, ldx, V, nrhs);
+  k_fwd_large_gather<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, 0, st>>>(F, list, dinv, X, ldx, V, nrhs,
+                                                                                    fused ? 0 : 1);
+  if (fused) {                    // the level's steps as one launch (single right-hand side)
+    if (launches) *launches += 1;
+    return;
+  }
   const int steps = ceil_div(max_nc, kSolveB);
   if (nrhs >= kMrhsMin) {
     const int rtiles = ceil_div(nrhs, kMT), rows = std::max(1, ceil_div(max_nf, kMT));
@@ -2732,9 +2956,13 @@ void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int ma
 template <typename T>
 void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
                       const T* dinv, T* X, int64_t ldx, T* V, T* scratch, int32_t* cnt, int nrhs, cudaStream_t st,
-                      int64_t* launches, bool pdl) {
+                      int64_t* launches, bool pdl, bool fused) {
   if (count <= 0) return;
   k_bwd_large_gather<T><<<dim3(count, nrhs >= kMrhsMin ? nrhs : 1), 256, 0, st>>>(F, list, X, ldx, V, nrhs);
+  if (fused) {
+    if (launches) *launches += 1;
+    return;
+  }
   const int steps = ceil_div(max_nc, kSolveB);
   const int chunks = std::max(1, ceil_div(max_nf, kSolveRows));
   if (nrhs >= kMrhsMin) {
@@ -2753,6 +2981,15 @@ void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int ma
     launch_k(k_bwd_large_step<T>, dim3(chunks, count), dim3(256), 0, st, pdl, F, list, s, panel, dinv, X, ldx, V,
              scratch, cnt, nrhs);
   if (launches) *launches += 1 + steps;
+}
+template <typename T>
+void launch_large_fused(const DevFronts& F, const int4* tasks, int ntask, bool backward, int32_t* ticket,
+                        int32_t* flags, int32_t* expired, const T* panel, const T* dinv, T* X, T* V, cudaStream_t st) {
+  if (ntask <= 0) return;
+  if (backward)
+    k_bwd_large_fused<T><<<ntask, 256, 0, st>>>(F, tasks, ntask, ticket, flags, expired, panel, dinv, X, V);
+  else
+    k_fwd_large_fused<T><<<ntask, 256, 0, st>>>(F, tasks, ntask, ticket, flags, expired, panel, dinv, X, V);
 }
 
 template <typename T>
@@ -2869,9 +3106,11 @@ void launch_remap_int(const int32_t* map, int32_t* a, int64_t n, cudaStream_t st
   template void launch_bwd_small<T>(const DevFronts&, const int32_t*, int, int, const T*, T*, int64_t, int,         \
                                     cudaStream_t);                                                                 \
   template void launch_fwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
-                                    int64_t, T*, int32_t*, int, cudaStream_t, int64_t*, bool);                     \
+                                    int64_t, T*, int32_t*, int, cudaStream_t, int64_t*, bool, bool);               \
   template void launch_bwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
-                                    int64_t, T*, T*, int32_t*, int, cudaStream_t, int64_t*, bool);                 \
+                                    int64_t, T*, T*, int32_t*, int, cudaStream_t, int64_t*, bool, bool);           \
+  template void launch_large_fused<T>(const DevFronts&, const int4*, int, bool, int32_t*, int32_t*, int32_t*,      \
+                                      const T*, const T*, T*, T*, cudaStream_t);                                   \
   template void launch_permute_in<T>(const double*, int64_t, const int32_t*, T*, int64_t, int64_t, int,            \
                                      cudaStream_t);                                                                \
   template void launch_permute_out<T>(const T*, int64_t, const int32_t*, double*, int64_t, int64_t, int,           \

@@ -196,15 +196,23 @@ template <typename T>
 void launch_bwd_small(const DevFronts& F, const int32_t* list, int count, int nf_max, const T* panel, T* X,
                       int64_t ldx, int nrhs, cudaStream_t st);
 // Large fronts: dinv holds the inverted 128 x 128 diagonal blocks the factorization kept (DevFronts::d_off).
+// fused: only the gather runs here (single right-hand side; launch_large_fused does the steps)
 template <typename T>
 void launch_fwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
                       const T* dinv, T* X, int64_t ldx, T* V, int32_t* cnt, int nrhs, cudaStream_t st,
-                      int64_t* launches, bool pdl);
+                      int64_t* launches, bool pdl, bool fused = false);
 // cnt: one zero-initialised ticket per list slot (left zero again on exit)
 template <typename T>
 void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int max_nc, int max_nf, const T* panel,
                       const T* dinv, T* X, int64_t ldx, T* V, T* scratch, int32_t* cnt, int nrhs, cudaStream_t st,
-                      int64_t* launches, bool pdl);
+                      int64_t* launches, bool pdl, bool fused = false);
+// A level's single-RHS large-front sweep as one launch over its task list (4 ints per task:
+// front, code, flag base, 0; forward code >= 0: diagonal block, < 0: rest rows chunk -1 - code;
+// backward code: column block).  ticket: zero before the launch; flags: zero before the sweep
+// (one per front and panel step); expired: raised when a bounded wait gives up.
+template <typename T>
+void launch_large_fused(const DevFronts& F, const int4* tasks, int ntask, bool backward, int32_t* ticket,
+                        int32_t* flags, int32_t* expired, const T* panel, const T* dinv, T* X, T* V, cudaStream_t st);
 // pdl: the single-RHS step kernels go out with programmatic dependent launch
 // (each waits for its predecessor before reading the sweep's vectors)
 

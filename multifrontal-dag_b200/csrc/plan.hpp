@@ -57,6 +57,9 @@ struct LevelPlan {
   std::vector<LaunchList> steps;     // per panel step: prefix of `large`; param = TRSM row blocks,
                                      // param2 = 128-tiles, param3 = 64-tiles of the trailing triangle
   std::vector<LaunchList> solve_steps;
+  // single-RHS large-front solve in one launch per sweep: task lists (4 ints per task)
+  // in the solve task pool, forward and backward
+  LaunchList fwd_tasks, bwd_tasks;
   int32_t large_max_nf = 0;
   int64_t large_zero_elems = 0;
 };

@@ -960,10 +960,13 @@ __global__ void __launch_bounds__(256) k_trsm2(DevFronts F, const int32_t* list,
   }
   pdl_wait();
   pdl_trigger();
-  for (int e = threadIdx.x; e < kFactB * kp; e += blockDim.x) {
-    const int k = e / kFactB, n = e - k * kFactB;
-    const bool v = k < w && n < w;
-    cp_async_t(&Bs[k * kTr2LdB + n], v ? Li + n + (size_t)k * kFactB : Li, v);
+  // Li in 16-byte copies: the block is 16-byte aligned, rows of 128 elements, and zero
+  // outside its lower w x w part (so the rows k < kp copy whole)
+  constexpr int kVec = 16 / (int)sizeof(T);
+  for (int e = threadIdx.x; e < kFactB / kVec * kp; e += blockDim.x) {
+    const int k = e / (kFactB / kVec), n = (e - k * (kFactB / kVec)) * kVec;
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(&Bs[k * kTr2LdB + n]);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(Li + n + (size_t)k * kFactB));
   }
   cp_async_commit();
   cp_async_wait<0>();

@@ -173,6 +173,8 @@ struct mfd_handle {
   std::vector<int32_t> h_lists;
   std::vector<int32_t> h_stasks;                    // fused single-RHS solve tasks, 4 ints each
   int32_t solve_flags = 0;                          // per front and panel step, one sweep's worth
+  int64_t bw_part_elems = 0;                        // backward sweep partial sums, largest level
+  void* d_bwpart = nullptr;                         // T, the backward sweep's partial sums
   std::vector<int> small_bins;
   int64_t panel_elems = 0, upool_elems = 0, v_elems = 0, s_elems = 0, dinv_elems = 0;
   int64_t q_elems = 0;                              // packed FP32 update operands of one step parity
@@ -237,7 +239,7 @@ struct mfd_handle {
     for (auto& kv : g_solve) cudaGraphExecDestroy(kv.second);
     for (auto& kv : g_ir) cudaGraphExecDestroy(kv.second);
     if (bst) cudaStreamDestroy(bst);
-    for (void* p : {d_panel, d_upool, d_diag, d_X, d_V, d_S, static_cast<void*>(d_q)})
+    for (void* p : {d_panel, d_upool, d_diag, d_X, d_V, d_S, static_cast<void*>(d_q), d_bwpart})
       if (p) cudaFree(p);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -391,6 +393,7 @@ int build_plan(mfd_handle* h) {
   h->h_lists.clear();
   h->h_stasks.clear();
   h->solve_flags = 0;
+  h->bw_part_elems = 0;
   h->max_large_count = 0;
   std::vector<std::vector<int32_t>> lev_fronts(nlev);
   for (int32_t g = 0; g < nfr; ++g) lev_fronts[h->fronts[g].level].push_back(g);
@@ -505,10 +508,31 @@ int build_plan(mfd_handle* h) {
       for (size_t k = 0; k < large.size(); ++k)
         for (int j = 0; j * kFactB < h->fronts[large[k]].nr; ++j) push_task(large[k], -1 - j, fbase[k]);
       L.fwd_tasks.count = (int32_t)(h->h_stasks.size() / 4) - L.fwd_tasks.off;
+      // backward: first the partial sums over the update rows (chunk j of kBwdRestRows rows
+      // against column block s, no waits), then the column-block tasks from the last step down;
+      // the fourth int is the front's partial-sum base in the level's scratch
       L.bwd_tasks.off = (int32_t)(h->h_stasks.size() / 4);
+      std::vector<int32_t> pbase(large.size());
+      int64_t pl = 0;
+      for (size_t k = 0; k < large.size(); ++k) {
+        const HostFront& fr = h->fronts[large[k]];
+        const int ns = (fr.nc + kFactB - 1) / kFactB, nch = (fr.nr + kBwdRestRows - 1) / kBwdRestRows;
+        pbase[k] = (int32_t)pl;
+        pl += (int64_t)ns * nch * kFactB;
+      }
+      h->bw_part_elems = std::max(h->bw_part_elems, pl);
+      auto push_bwd = [&](int32_t g, int32_t code, int32_t flag, int32_t pb) {
+        h->h_stasks.insert(h->h_stasks.end(), {g, code, flag, pb});
+      };
+      for (size_t k = 0; k < large.size(); ++k) {
+        const HostFront& fr = h->fronts[large[k]];
+        const int ns = (fr.nc + kFactB - 1) / kFactB, nch = (fr.nr + kBwdRestRows - 1) / kBwdRestRows;
+        for (int s = 0; s < ns; ++s)
+          for (int j = 0; j < nch; ++j) push_bwd(large[k], -1 - ((s << 16) | j), fbase[k], pbase[k]);
+      }
       for (int s = steps - 1; s >= 0; --s)
         for (size_t k = 0; k < large.size(); ++k)
-          if (h->fronts[large[k]].nc > s * kFactB) push_task(large[k], s, fbase[k]);
+          if (h->fronts[large[k]].nc > s * kFactB) push_bwd(large[k], s, fbase[k], pbase[k]);
       L.bwd_tasks.count = (int32_t)(h->h_stasks.size() / 4) - L.bwd_tasks.off;
     }
   }
@@ -549,7 +573,8 @@ int upload_plan(mfd_handle* h) {
   CK(h->d_q_off.upload(qoff, st));
   CK(h->d_lists.upload(h->h_lists, st));
   if (!h->h_stasks.empty()) CK(h->d_stasks.upload(h->h_stasks, st));
-  CK(h->d_ssync.alloc(1 + 2 * h->levels.size() + 2 * (size_t)h->solve_flags));
+  // [0] expiry, 2 tickets per level, forward flags, backward flags, backward update-row counters
+  CK(h->d_ssync.alloc(1 + 2 * h->levels.size() + 3 * (size_t)h->solve_flags));
   CK(cudaMemsetAsync(h->d_ssync.p, 0, sizeof(int32_t) * h->d_ssync.n, st));
   CK(h->d_a_src.alloc(h->nnz_total));
   CK(h->d_a_pos.alloc(h->nnz_total));
@@ -721,6 +746,7 @@ int upload_plan(mfd_handle* h) {
   CK(cudaMalloc(&h->d_panel, (std::max<int64_t>(h->panel_elems, 1) + 32) * esz));
   CK(cudaMalloc(&h->d_upool, std::max<int64_t>(h->upool_elems, 1) * esz));
   CK(cudaMalloc(&h->d_diag, (size_t)std::max<int64_t>(h->dinv_elems, 1) * esz));
+  CK(cudaMalloc(&h->d_bwpart, (size_t)std::max<int64_t>(h->bw_part_elems, 1) * esz));
   if (h->fp32 && h->q_elems > 0) {
     CK(cudaMalloc(&h->d_q, (size_t)(2 * h->q_elems) * sizeof(float)));
     // rows past a front's last row are never written and only reach discarded outputs; zero keeps them finite
@@ -1112,7 +1138,8 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
         if (fused) {
           const size_t lv = &L - h->levels.data();
           launch_large_fused<T>(F, stasks + L.bwd_tasks.off, L.bwd_tasks.count, true, ssync + 2 + 2 * lv, bwd_flags,
-                                ssync, panel, dinv, X, V, st);
+                                ssync, panel, dinv, X, V, st, static_cast<T*>(h->d_bwpart),
+                                bwd_flags + h->solve_flags);
           ++n;
         }
       });

@@ -2101,11 +2101,27 @@ __device__ __forceinline__ void bwd_rows_acc(const T* P, int nf, int c0, int w, 
   }
 }
 
+// butterfly transpose-reduce of 16 per-lane column sums: lane l ends with column (l mod 16)'s sum
+template <typename T>
+__device__ __forceinline__ T transpose_reduce16(T (&acc)[16], int lane) {
+#pragma unroll
+  for (int sft = 8; sft >= 1; sft >>= 1) {
+    const bool up = (lane & sft) != 0;
+#pragma unroll
+    for (int j = 0; j < sft; ++j) {
+      const T send = up ? acc[j] : acc[j + sft];
+      const T keep = up ? acc[j + sft] : acc[j];
+      acc[j] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
+    }
+  }
+  return acc[0] + __shfl_xor_sync(0xffffffffu, acc[0], 16);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_bwd_large_fused(DevFronts F, const int4* __restrict__ tasks, int ntask,
                                                          int32_t* ticket, int32_t* flags, int32_t* expired,
                                                          const T* __restrict__ panel, const T* __restrict__ dinv,
-                                                         T* X, T* V) {
+                                                         T* X, T* V, T* part, int32_t* counters) {
   __shared__ int sh_t, sh_ok;
   __shared__ T ts[kSolveB];
   if (threadIdx.x == 0) sh_t = atomicAdd(ticket, 1);
@@ -2113,18 +2129,34 @@ __global__ void __launch_bounds__(256) k_bwd_large_fused(DevFronts F, const int4
   const int t = sh_t;
   if (t >= ntask) return;
   const int4 tk = tasks[t];
-  const int f = tk.x, s = tk.y;
+  const int f = tk.x;
   int32_t* fl = flags + tk.z;
-  const int nc = F.nc[f], nf = nc + F.nr[f];
+  const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
   const int nsteps = (nc + kSolveB - 1) / kSolveB;
-  const int c0 = s * kSolveB, w = min(kSolveB, nc - c0);
+  const int nch = (nr + kBwdRestRows - 1) / kBwdRestRows;
   const T* P = panel + F.panel_off[f];
   T* Vf = V + F.v_off[f];
+  T* Pt = part + tk.w;                        // the front's partial sums: [step][chunk][128]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wc = 16 * warp;
   T acc[16];
 #pragma unroll
   for (int j = 0; j < 16; ++j) acc[j] = T(0);
-  bwd_rows_acc(P, nf, c0, w, nc, nf, Vf, false, wc, lane, acc);            // update rows: x gathered
+  if (tk.y < 0) {                             // update-row chunk j against column block s (x gathered)
+    const int code = -1 - tk.y, s = code >> 16, j = code & 0xffff;
+    const int c0 = s * kSolveB, w = min(kSolveB, nc - c0);
+    const int ra = nc + j * kBwdRestRows;
+    bwd_rows_acc(P, nf, c0, w, ra, min(nf, ra + kBwdRestRows), Vf, false, wc, lane, acc);
+    const T sum = transpose_reduce16(acc, lane);
+    if (lane < 16) Pt[((size_t)s * nch + j) * kSolveB + wc + lane] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(&counters[tk.z + s], 1);
+    }
+    return;
+  }
+  const int s = tk.y;
+  const int c0 = s * kSolveB, w = min(kSolveB, nc - c0);
   for (int b = nsteps - 1; b > s; --b) {                                   // later diagonal blocks
     const int ra = b * kSolveB, rb = min(nc, ra + kSolveB);
     T l[4][16];
@@ -2144,21 +2176,33 @@ __global__ void __launch_bounds__(256) k_bwd_large_fused(DevFronts F, const int4
       for (int j = 0; j < 16; ++j) acc[j] += l[q][j] * xv;
     }
   }
-  // butterfly transpose-reduce: lane l ends with column wc + (l mod 16)'s sum
-#pragma unroll
-  for (int sft = 8; sft >= 1; sft >>= 1) {
-    const bool up = (lane & sft) != 0;
-#pragma unroll
-    for (int j = 0; j < sft; ++j) {
-      const T send = up ? acc[j] : acc[j + sft];
-      const T keep = up ? acc[j + sft] : acc[j];
-      acc[j] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
+  const T dsum = transpose_reduce16(acc, lane);           // lane l: column wc + (l mod 16), diagonal blocks
+  // the update rows' partial sums, chunk by chunk in order, once every chunk task has counted in
+  if (nch > 0) {
+    if (threadIdx.x == 0) {
+      int ok = 1;
+      const int32_t* cnt = counters + tk.z + s;
+      if (ld_acquire_i32(cnt) < nch) {
+        const long long t0 = clock64();
+        while (ld_acquire_i32(cnt) < nch) {
+          if (clock64() - t0 > kSolveWaitLimit || ld_acquire_i32(expired) != 0) {
+            ok = 0;
+            atomicExch(expired, 1);
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      sh_ok = ok;
     }
+    __syncthreads();
+    if (!sh_ok) return;
   }
-  acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 16);
   if (lane < 16) {
     const int c = wc + lane;
-    ts[c] = c < w ? Vf[c0 + c] - acc[0] : T(0);
+    T rsum = T(0);
+    for (int j = 0; j < nch; ++j) rsum += __ldcg(&Pt[((size_t)s * nch + j) * kSolveB + c]);
+    ts[c] = c < w ? Vf[c0 + c] - (rsum + dsum) : T(0);
   }
   __syncthreads();
   // x = Li^T t: column i of Li against t, lanes over k (coalesced), 16 columns per warp
@@ -3037,10 +3081,12 @@ void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int ma
 }
 template <typename T>
 void launch_large_fused(const DevFronts& F, const int4* tasks, int ntask, bool backward, int32_t* ticket,
-                        int32_t* flags, int32_t* expired, const T* panel, const T* dinv, T* X, T* V, cudaStream_t st) {
+                        int32_t* flags, int32_t* expired, const T* panel, const T* dinv, T* X, T* V, cudaStream_t st,
+                        T* part, int32_t* counters) {
   if (ntask <= 0) return;
   if (backward)
-    k_bwd_large_fused<T><<<ntask, 256, 0, st>>>(F, tasks, ntask, ticket, flags, expired, panel, dinv, X, V);
+    k_bwd_large_fused<T><<<ntask, 256, 0, st>>>(F, tasks, ntask, ticket, flags, expired, panel, dinv, X, V, part,
+                                                counters);
   else
     k_fwd_large_fused<T><<<ntask, 256, 0, st>>>(F, tasks, ntask, ticket, flags, expired, panel, dinv, X, V);
 }
@@ -3163,7 +3209,7 @@ void launch_remap_int(const int32_t* map, int32_t* a, int64_t n, cudaStream_t st
   template void launch_bwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
                                     int64_t, T*, T*, int32_t*, int, cudaStream_t, int64_t*, bool, bool);           \
   template void launch_large_fused<T>(const DevFronts&, const int4*, int, bool, int32_t*, int32_t*, int32_t*,      \
-                                      const T*, const T*, T*, T*, cudaStream_t);                                   \
+                                      const T*, const T*, T*, T*, cudaStream_t, T*, int32_t*);                     \
   template void launch_permute_in<T>(const double*, int64_t, const int32_t*, T*, int64_t, int64_t, int,            \
                                      cudaStream_t);                                                                \
   template void launch_permute_out<T>(const T*, int64_t, const int32_t*, double*, int64_t, int64_t, int,           \

@@ -41,6 +41,7 @@ int fail(int code, const std::string& msg) {
 
 constexpr int64_t kAlign = 32;  // elements; keeps every front 256-byte aligned in FP64
 constexpr int kResMulti = 4;     // from this many right-hand sides on, one multi-column residual per IR sweep
+constexpr int kPotrfSplitMin = 148;   // fronts in a panel step above which POTRF launches per width class
 constexpr int kDeferDefault = 1; // panel steps per deferred trailing update (measured: deferring costs time)
 int64_t align_up(int64_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
@@ -490,6 +491,12 @@ int build_plan(mfd_handle* h) {
       ll.param2 = tiles128;
       ll.param3 = tiles64;
       L.steps.push_back(ll);
+      std::array<int32_t, 4> cls{0, 0, 0, 0};   // block widths are non-increasing along the nc-sorted list
+      for (int k = 0; k < cntf; ++k) {
+        const int w = std::min(kFactB, h->fronts[large[k]].nc - s * kFactB);
+        ++cls[4 - (w + 31) / 32];
+      }
+      L.potrf_cls.push_back(cls);
     }
     // single-RHS solve tasks of the level, in dependency order (see launch_large_fused)
     {
@@ -975,8 +982,12 @@ int64_t enqueue_factor(mfd_handle* h, cudaStream_t st) {
         }
       };
       record(h, st, MFD_K_PANEL, pf, pb,
-             [&] { launch_potrf<T>(F, lists + p.off, p.count, (int)s, panel, diag, h->d_info.p, st, pdl, 0,
-                                   h->d_info.p + 3); });
+             [&] {
+               // many fronts: one launch per sub-block class (narrow blocks fit many CTAs per SM);
+               // a few: one launch (measured: the extra launches on the panel chain cost more)
+               launch_potrf<T>(F, lists + p.off, p.count, (int)s, panel, diag, h->d_info.p, st, pdl, 0,
+                               h->d_info.p + 3, p.count > kPotrfSplitMin ? L.potrf_cls[s].data() : nullptr);
+             });
       record(h, st, MFD_K_TRSM, tf, tb, [&] {
         launch_trsm<T>(F, lists + p.off, p.count, (int)s, p.param, panel, diag, kind == 1 ? 1 : 0, st, pdl,
                        tcq ? h->d_q + (s & 1) * h->q_elems : nullptr);

@@ -599,13 +599,29 @@ __global__ void __launch_bounds__(256) k_extend_add_ilp(DevFronts F, const int32
 // persistent blocks are zeroed at allocation and written on that part only)
 // to linv.  A non-positive pivot records its 1-based column in info (atomic
 // min) and continues with pivot 1.
-constexpr int kPotrfThreads = 256;
 constexpr int kPSub = 32;
 constexpr int kPLd = kFactB + 4;   // 132: ld = 4 mod 16 doubles keeps DMMA fragment loads conflict-free
 constexpr int kDLd = kPSub + 4;    // 36
-constexpr size_t kPotrfSmem =
-    sizeof(double) * ((size_t)kFactB * kPLd + (size_t)(kFactB / kPSub) * kPSub * kDLd +
-                      (size_t)(kFactB / kPSub - 1) * kPSub * kDLd + kFactB + 2 * kPSub);
+// The kernel is instantiated per number of 32-wide sub-blocks NSB (the block
+// width w <= 32 NSB): shared memory for 32 NSB columns of S (ld kPLd), NSB
+// inverse blocks and NSB - 1 scratch blocks; 32 x {1, 2, 4, 8} threads, the
+// most any phase uses (sub-panel TRSM: NSB - 1 warps, trailing tiles, inverse:
+// 2 (NSB - 1) warps), so narrow panels fit many fronts per SM.
+// scratch blocks Yv: NSB - 1 for the inverse, at least one (the FP32 pivot chain's
+// 32 x 33 float copy of the sub-block lives there)
+template <int NSB>
+__host__ __device__ constexpr int potrf_yblocks() {
+  return NSB > 1 ? NSB - 1 : 1;
+}
+template <int NSB>
+__host__ __device__ constexpr size_t potrf_smem() {
+  return sizeof(double) * ((size_t)kPSub * NSB * kPLd + (size_t)NSB * kPSub * kDLd +
+                           (size_t)potrf_yblocks<NSB>() * kPSub * kDLd + kFactB + 2 * kPSub);
+}
+template <int NSB>
+__host__ __device__ constexpr int potrf_threads() {
+  return NSB == 1 ? 32 : NSB == 2 ? 64 : NSB == 3 ? 128 : 256;
+}
 
 
 // One warp: acc(8 MF x 32) += A(8 MF x K) B(K x 32), K a multiple of 4, operands
@@ -788,22 +804,23 @@ __device__ __forceinline__ T* inv_block(const DevFronts& F, T* linv, int f, int 
 
 // info_stride 0: every front reports into info[0]; 1: list slot i reports into info[i].
 // fallbacks (may be null): counts the FP32 sub-blocks redone in FP64.
-template <typename T>
-__global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const int32_t* list, int step, T* panel,
-                                                            T* linv, int32_t* info, int info_stride,
-                                                            int32_t* fallbacks) {
-  constexpr int B = kFactB;
+template <typename T, int NSB>
+__global__ void __launch_bounds__(potrf_threads<NSB>(), 1) k_potrf(DevFronts F, const int32_t* list, int step,
+                                                                   T* panel, T* linv, int32_t* info, int info_stride,
+                                                                   int32_t* fallbacks) {
+  constexpr int B = kPSub * NSB;                             // the block's capacity (w <= B)
+  constexpr int NT = potrf_threads<NSB>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* S = reinterpret_cast<double*>(smem_raw);
-  double* Dv = S + (size_t)B * kPLd;                         // 4 blocks of kPSub x kDLd
-  double* Yv = Dv + (size_t)(B / kPSub) * kPSub * kDLd;       // 3 blocks
-  double* rq = Yv + (size_t)(B / kPSub - 1) * kPSub * kDLd;   // B
-  double* cbuf = rq + B;                                      // 2 x kPSub
+  double* Dv = S + (size_t)B * kPLd;                         // NSB blocks of kPSub x kDLd
+  double* Yv = Dv + (size_t)NSB * kPSub * kDLd;               // potrf_yblocks<NSB>() blocks
+  double* rq = Yv + (size_t)potrf_yblocks<NSB>() * kPSub * kDLd;   // kFactB
+  double* cbuf = rq + kFactB;                                 // 2 x kPSub
   const int f = list[blockIdx.x];
   const int nc = F.nc[f], nf = nc + F.nr[f];
-  const int c0 = step * B;
+  const int c0 = step * kFactB;
   if (c0 >= nc) return;
-  const int w = min(B, nc - c0);
+  const int w = min(kFactB, nc - c0);                       // <= B by the launch's choice of NSB
   const int nsb = (w + kPSub - 1) / kPSub, wp = nsb * kPSub;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   T* P = panel + F.panel_off[f];
@@ -812,7 +829,7 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
   // ---- load the lower w x w block, identity on the padding ----
   if constexpr (sizeof(T) == 8) {
     // asynchronous 8-byte copies, all in flight at once; out-of-block entries zero-filled
-    for (int e = tid; e < B * B; e += kPotrfThreads) {
+    for (int e = tid; e < B * B; e += NT) {
       const int i = e % B, j = e / B;
       if (i < wp && j < wp) {
         if (i == j && i >= w) {
@@ -827,16 +844,17 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
     cp_async_wait<0>();
   } else {
     // FP32 storage: 4-byte copies into a float staging block (the D / Y / rq /
-    // cbuf area, 66 KB, is free until the first sub-block), then widened into S
+    // cbuf area, larger than B x B floats, is free until the first sub-block),
+    // then widened into S
     float* Fs = reinterpret_cast<float*>(Dv);
-    for (int e = tid; e < B * B; e += kPotrfThreads) {
+    for (int e = tid; e < B * B; e += NT) {
       const int i = e % B, j = e / B;
       if (i < w && j < w && i >= j) cp_async_t(&Fs[e], (const float*)&P[(c0 + i) + (size_t)(c0 + j) * nf], true);
     }
     cp_async_commit();
     cp_async_wait<0>();
     __syncthreads();
-    for (int e = tid; e < B * B; e += kPotrfThreads) {
+    for (int e = tid; e < B * B; e += NT) {
       const int i = e % B, j = e / B;
       if (i < wp && j < wp) S[i + j * kPLd] = (i < w && j < w) ? (i >= j ? (double)Fs[e] : 0.0) : (i == j ? 1.0 : 0.0);
     }
@@ -872,7 +890,7 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
       acc_store(acc, S + r0 + o * kPLd, 1, kPLd, 1.0, lane);
     }
     __syncthreads();
-    for (int t = warp; t < rt * (rt + 1) / 2; t += kPotrfThreads / 32) {   // trailing lower tiles
+    for (int t = warp; t < rt * (rt + 1) / 2; t += NT / 32) {   // trailing lower tiles
       int ti = 0;
       while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
       const int tj = t - ti * (ti + 1) / 2;
@@ -916,15 +934,16 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
     __syncthreads();
   }
   // ---- write L11 to the panel and X to linv ----
-  for (int e = tid; e < B * B; e += kPotrfThreads) {
+  for (int e = tid; e < B * B; e += NT) {
     const int i = e % B, j = e / B;
     if (i < w && j < w && i >= j) P[(c0 + i) + (size_t)(c0 + j) * nf] = (T)S[i + j * kPLd];
   }
   // persistent blocks (d_off) were zeroed once: only their lower w x w part is written
   T* Li = inv_block(F, linv, f, step, blockIdx.x);
-  const bool full = F.d_off == nullptr;
-  for (int e = tid; e < B * B; e += kPotrfThreads) {
-    const int i = e % B, j = e / B;
+  const bool full = F.d_off == nullptr;                      // scratch blocks: the whole 128 x 128 block written
+  const int EB = full ? kFactB : B;
+  for (int e = tid; e < EB * EB; e += NT) {
+    const int i = e % EB, j = e / EB;
     const bool in = i < w && j < w && i >= j;
     if (!in && !full) continue;
     double v = 0.0;
@@ -932,7 +951,7 @@ __global__ void __launch_bounds__(kPotrfThreads, 1) k_potrf(DevFronts F, const i
       const int bi = i / kPSub, bj = j / kPSub;
       v = bi == bj ? Dv[(size_t)bi * kPSub * kDLd + (i - bi * kPSub) + (j - bj * kPSub) * kDLd] : S[j + i * kPLd];
     }
-    Li[e] = (T)v;
+    Li[i + (size_t)j * kFactB] = (T)v;
   }
 }
 
@@ -2876,7 +2895,10 @@ cudaError_t prepare_kernels() {
   chk(opt_in(k_small_front<double, true>)); chk(opt_in(k_small_front<float, true>));
   chk(opt_in(k_trsm2<double>)); chk(opt_in(k_trsm2<float>));
   chk(opt_in(k_update_dmma));
-  chk(opt_in(k_potrf<double>)); chk(opt_in(k_potrf<float>));
+  chk(opt_in(k_potrf<double, 4>)); chk(opt_in(k_potrf<float, 4>));
+  chk(opt_in(k_potrf<double, 3>)); chk(opt_in(k_potrf<float, 3>));
+  chk(opt_in(k_potrf<double, 2>)); chk(opt_in(k_potrf<float, 2>));
+  chk(opt_in(k_potrf<double, 1>)); chk(opt_in(k_potrf<float, 1>));
   chk(prepare_update_tc());
   chk(prepare_update_tcq());
   chk(opt_in(k_update_simt<double>)); chk(opt_in(k_update_simt<float>));
@@ -2948,10 +2970,26 @@ void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int m
 }
 template <typename T>
 void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
-                  cudaStream_t st, bool pdl, int info_stride, int32_t* fallbacks) {
+                  cudaStream_t st, bool pdl, int info_stride, int32_t* fallbacks, const int32_t* cls) {
   if (count <= 0) return;
-  launch_k(k_potrf<T>, dim3(count), dim3(kPotrfThreads), kPotrfSmem, st, pdl, F, list, step, panel, linv, info,
-           info_stride, fallbacks);
+  if (cls == nullptr) {                   // one launch, any block width
+    launch_k(k_potrf<T, 4>, dim3(count), dim3(potrf_threads<4>()), potrf_smem<4>(), st, pdl, F, list, step, panel,
+             linv, info, info_stride, fallbacks);
+    return;
+  }
+  // cls[k]: fronts of the list (in order, block widths non-increasing) whose block needs 4 - k sub-blocks;
+  // the list slots of a launch are offset, so this form is for persistent inverse blocks (F.d_off)
+  int off = 0;
+  auto go = [&](auto kern, int nt, size_t smem, int cnt) {
+    if (cnt > 0)
+      launch_k(kern, dim3(cnt), dim3(nt), smem, st, pdl, F, list + off, step, panel, linv, info, info_stride,
+               fallbacks);
+    off += cnt;
+  };
+  go(k_potrf<T, 4>, potrf_threads<4>(), potrf_smem<4>(), cls[0]);
+  go(k_potrf<T, 3>, potrf_threads<3>(), potrf_smem<3>(), cls[1]);
+  go(k_potrf<T, 2>, potrf_threads<2>(), potrf_smem<2>(), cls[2]);
+  go(k_potrf<T, 1>, potrf_threads<1>(), potrf_smem<1>(), cls[3]);
 }
 template <typename T>
 void launch_trsm(const DevFronts& F, const int32_t* list, int count, int step, int row_blocks, T* panel,
@@ -3195,7 +3233,7 @@ void launch_remap_int(const int32_t* map, int32_t* a, int64_t n, cudaStream_t st
                                          cudaStream_t);                                                            \
   template void launch_extend_add<T>(const DevFronts&, const int32_t*, int, int, T*, T*, cudaStream_t);             \
   template void launch_potrf<T>(const DevFronts&, const int32_t*, int, int, T*, T*, int32_t*, cudaStream_t, bool,  \
-                                int, int32_t*);                                                                    \
+                                int, int32_t*, const int32_t*);                                                    \
   template void launch_trsm<T>(const DevFronts&, const int32_t*, int, int, int, T*, const T*, int, cudaStream_t,   \
                                bool, float*);                                                                           \
   template int launch_update<T>(const DevFronts&, const int32_t*, int, int, int, int, T*, T*, int, cudaStream_t,    \

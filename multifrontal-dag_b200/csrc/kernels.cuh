@@ -139,8 +139,12 @@ void launch_extend_add(const DevFronts& F, const int32_t* list, int count, int m
 // FP32: the diagonal sub-blocks' pivot chains run in FP32 with an FP64 fallback on a small pivot;
 // fallbacks (may be null) counts the sub-blocks redone in FP64.
 template <typename T>
+// cls (may be null: one launch): four counts splitting the list, in order, into fronts whose
+// block needs 4, 3, 2, 1 sub-blocks of 32 columns, each class launched with its own (smaller)
+// shared memory and thread count; only for persistent inverse blocks (F.d_off).
 void launch_potrf(const DevFronts& F, const int32_t* list, int count, int step, T* panel, T* linv, int32_t* info,
-                  cudaStream_t st, bool pdl = false, int info_stride = 0, int32_t* fallbacks = nullptr);
+                  cudaStream_t st, bool pdl = false, int info_stride = 0, int32_t* fallbacks = nullptr,
+                  const int32_t* cls = nullptr);
 // q (FP32 only, may be null): also write the solved rows as packed TF32 operands of the
 // tensor-core update (packed_offset below), at q + F.q_off[f].
 template <typename T>

@@ -10,6 +10,7 @@
 //   vector pool : nf entries per front per right-hand side (solve work vectors)
 // Front positions 0..nc-1 are the supernode's columns, nc..nf-1 its L rows.
 #pragma once
+#include <array>
 #include <cstdint>
 #include <vector>
 
@@ -57,6 +58,9 @@ struct LevelPlan {
   std::vector<LaunchList> steps;     // per panel step: prefix of `large`; param = TRSM row blocks,
                                      // param2 = 128-tiles, param3 = 64-tiles of the trailing triangle
   std::vector<LaunchList> solve_steps;
+  // per panel step: how many fronts of the step's list (in order) need 4, 3, 2, 1
+  // sub-blocks of 32 columns in the diagonal-block POTRF
+  std::vector<std::array<int32_t, 4>> potrf_cls;
   // single-RHS large-front solve in one launch per sweep: task lists (4 ints per task)
   // in the solve task pool, forward and backward
   LaunchList fwd_tasks, bwd_tasks;

@@ -273,7 +273,11 @@ int mfd_get_profile(mfd_handle *h, int32_t kind, mfd_kernel_profile *out);
  * expired wait raises the handle's error flag and the kernel returns, so the
  * next mfd_factorize returns MFD_E_TIMEOUT (no GPU fault: every wait is
  * bounded).  Disable it and the handle factors normally again.  FP64 handles
- * and fronts that use no tensor-core update are unaffected. */
+ * and fronts that use no tensor-core update factor normally.  While enabled,
+ * the single-RHS large-front solve sweeps' device waits (one launch per level,
+ * tasks waiting on other tasks' flags) likewise wait for a value nothing
+ * writes, with a ~1 ms limit: mfd_solve returns MFD_E_TIMEOUT, and solves
+ * normally once the request is withdrawn. */
 int mfd_test_expire_waits(mfd_handle *h, int32_t enable);
 
 int mfd_destroy(mfd_handle *h);

@@ -1122,7 +1122,7 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
         if (fused) {
           const size_t lv = &L - h->levels.data();
           launch_large_fused<T>(F, stasks + L.fwd_tasks.off, L.fwd_tasks.count, false, ssync + 1 + 2 * lv, fwd_flags,
-                                ssync, panel, dinv, X, V, st);
+                                ssync, panel, dinv, X, V, st, h->d_info.p + 2);
           ++n;
         }
       });
@@ -1151,7 +1151,7 @@ int64_t enqueue_solve_core(mfd_handle* h, int nrhs, cudaStream_t st) {
         if (fused) {
           const size_t lv = &L - h->levels.data();
           launch_large_fused<T>(F, stasks + L.bwd_tasks.off, L.bwd_tasks.count, true, ssync + 2 + 2 * lv, bwd_flags,
-                                ssync, panel, dinv, X, V, st, static_cast<T*>(h->d_bwpart),
+                                ssync, panel, dinv, X, V, st, h->d_info.p + 2, static_cast<T*>(h->d_bwpart),
                                 bwd_flags + h->solve_flags);
           ++n;
         }
@@ -1361,6 +1361,7 @@ int do_solve(mfd_handle* h, double* b, int nrhs, int64_t ldb, mfd_report* rep) {
     CK(cudaMemcpy2DAsync(h->d_b.p, sizeof(double) * n, b, sizeof(double) * ldb, sizeof(double) * n, nrhs,
                          dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
   }
+  launch_fill_int(h->d_info.p + 2, h->expire_waits ? 1 : 0, 1, st);   // test request (mfd_test_expire_waits)
   CK(cudaEventRecord(h->ev0, st));
   int iters = 0;
   double bwd = 0;

@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 #include <type_traits>
 
@@ -2011,15 +2012,20 @@ __device__ __forceinline__ int ld_acquire_i32(const int32_t* p) {
 __device__ __forceinline__ void st_release_i32(int32_t* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-// thread 0 waits for *flag != 0 (bounded; gives up at once when another CTA's
-// wait expired); the result is the CTA's
-__device__ __forceinline__ bool cta_wait_flag(const int32_t* flag, int32_t* expired, int* sh_ok) {
+constexpr long long kSolveProbeLimit = 1ll << 21;   // the test request's wait (~1 ms)
+// thread 0 waits for *flag >= need (bounded; gives up at once when another
+// CTA's wait expired); the result is the CTA's.  probe (a test request): the
+// wait is for a value no producer writes, with a ~1 ms limit, so it expires.
+__device__ __forceinline__ bool cta_wait_flag(const int32_t* flag, int32_t* expired, int* sh_ok, bool probe,
+                                              int need = 1) {
   if (threadIdx.x == 0) {
     int ok = 1;
-    if (ld_acquire_i32(flag) == 0) {
+    if (probe) need = INT_MAX;
+    const long long limit = probe ? kSolveProbeLimit : kSolveWaitLimit;
+    if (ld_acquire_i32(flag) < need) {
       const long long t0 = clock64();
-      while (ld_acquire_i32(flag) == 0) {
-        if (clock64() - t0 > kSolveWaitLimit || ld_acquire_i32(expired) != 0) {
+      while (ld_acquire_i32(flag) < need) {
+        if (clock64() - t0 > limit || ld_acquire_i32(expired) != 0) {
           ok = 0;
           atomicExch(expired, 1);
           break;
@@ -2040,7 +2046,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_fwd_large_fused(DevFronts F, const int4* __restrict__ tasks, int ntask,
                                                          int32_t* ticket, int32_t* flags, int32_t* expired,
                                                          const T* __restrict__ panel, const T* __restrict__ dinv,
-                                                         T* X, T* V) {
+                                                         T* X, T* V, const int32_t* test_req) {
   __shared__ int sh_t, sh_ok;
   __shared__ T ys[kSolveB];
   __shared__ T part[kFuseRows];
@@ -2051,6 +2057,7 @@ __global__ void __launch_bounds__(256) k_fwd_large_fused(DevFronts F, const int4
   const int4 tk = tasks[t];
   const int f = tk.x, code = tk.y;
   int32_t* fl = flags + tk.z;
+  const bool probe = *test_req != 0;
   const int nc = F.nc[f], nf = nc + F.nr[f];
   const int r0 = code >= 0 ? code * kSolveB : nc + (-1 - code) * kFuseRows;
   const int r1 = code >= 0 ? min(nc, r0 + kSolveB) : min(nf, r0 + kFuseRows);
@@ -2067,7 +2074,7 @@ __global__ void __launch_bounds__(256) k_fwd_large_fused(DevFronts F, const int4
     const T* pc = P + (valid ? i : 0) + (size_t)(c0 + 64 * h) * nf;
 #pragma unroll
     for (int k = 0; k < 64; ++k) l[k] = (valid && 64 * h + k < w) ? pc[(size_t)k * nf] : T(0);
-    if (!cta_wait_flag(fl + s, expired, &sh_ok)) return;
+    if (!cta_wait_flag(fl + s, expired, &sh_ok, probe)) return;
     if (tid < kSolveB) ys[tid] = tid < w ? __ldcg(&Vf[c0 + tid]) : T(0);
     __syncthreads();
 #pragma unroll
@@ -2140,7 +2147,8 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_bwd_large_fused(DevFronts F, const int4* __restrict__ tasks, int ntask,
                                                          int32_t* ticket, int32_t* flags, int32_t* expired,
                                                          const T* __restrict__ panel, const T* __restrict__ dinv,
-                                                         T* X, T* V, T* part, int32_t* counters) {
+                                                         T* X, T* V, T* part, int32_t* counters,
+                                                         const int32_t* test_req) {
   __shared__ int sh_t, sh_ok;
   __shared__ T ts[kSolveB];
   if (threadIdx.x == 0) sh_t = atomicAdd(ticket, 1);
@@ -2150,6 +2158,7 @@ __global__ void __launch_bounds__(256) k_bwd_large_fused(DevFronts F, const int4
   const int4 tk = tasks[t];
   const int f = tk.x;
   int32_t* fl = flags + tk.z;
+  const bool probe = *test_req != 0;
   const int nc = F.nc[f], nr = F.nr[f], nf = nc + nr;
   const int nsteps = (nc + kSolveB - 1) / kSolveB;
   const int nch = (nr + kBwdRestRows - 1) / kBwdRestRows;
@@ -2186,7 +2195,7 @@ __global__ void __launch_bounds__(256) k_bwd_large_fused(DevFronts F, const int4
 #pragma unroll
       for (int j = 0; j < 16; ++j) l[q][j] = (r < rb && wc + j < w) ? pr[(size_t)j * nf] : T(0);
     }
-    if (!cta_wait_flag(fl + b, expired, &sh_ok)) return;
+    if (!cta_wait_flag(fl + b, expired, &sh_ok, probe)) return;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int r = ra + lane + 32 * q;
@@ -2197,26 +2206,7 @@ __global__ void __launch_bounds__(256) k_bwd_large_fused(DevFronts F, const int4
   }
   const T dsum = transpose_reduce16(acc, lane);           // lane l: column wc + (l mod 16), diagonal blocks
   // the update rows' partial sums, chunk by chunk in order, once every chunk task has counted in
-  if (nch > 0) {
-    if (threadIdx.x == 0) {
-      int ok = 1;
-      const int32_t* cnt = counters + tk.z + s;
-      if (ld_acquire_i32(cnt) < nch) {
-        const long long t0 = clock64();
-        while (ld_acquire_i32(cnt) < nch) {
-          if (clock64() - t0 > kSolveWaitLimit || ld_acquire_i32(expired) != 0) {
-            ok = 0;
-            atomicExch(expired, 1);
-            break;
-          }
-          __nanosleep(32);
-        }
-      }
-      sh_ok = ok;
-    }
-    __syncthreads();
-    if (!sh_ok) return;
-  }
+  if (nch > 0 && !cta_wait_flag(counters + tk.z + s, expired, &sh_ok, probe, nch)) return;
   if (lane < 16) {
     const int c = wc + lane;
     T rsum = T(0);
@@ -3120,13 +3110,14 @@ void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int ma
 template <typename T>
 void launch_large_fused(const DevFronts& F, const int4* tasks, int ntask, bool backward, int32_t* ticket,
                         int32_t* flags, int32_t* expired, const T* panel, const T* dinv, T* X, T* V, cudaStream_t st,
-                        T* part, int32_t* counters) {
+                        const int32_t* test_req, T* part, int32_t* counters) {
   if (ntask <= 0) return;
   if (backward)
     k_bwd_large_fused<T><<<ntask, 256, 0, st>>>(F, tasks, ntask, ticket, flags, expired, panel, dinv, X, V, part,
-                                                counters);
+                                                counters, test_req);
   else
-    k_fwd_large_fused<T><<<ntask, 256, 0, st>>>(F, tasks, ntask, ticket, flags, expired, panel, dinv, X, V);
+    k_fwd_large_fused<T><<<ntask, 256, 0, st>>>(F, tasks, ntask, ticket, flags, expired, panel, dinv, X, V,
+                                                test_req);
 }
 
 template <typename T>
@@ -3247,7 +3238,7 @@ void launch_remap_int(const int32_t* map, int32_t* a, int64_t n, cudaStream_t st
   template void launch_bwd_large<T>(const DevFronts&, const int32_t*, int, int, int, const T*, const T*, T*,       \
                                     int64_t, T*, T*, int32_t*, int, cudaStream_t, int64_t*, bool, bool);           \
   template void launch_large_fused<T>(const DevFronts&, const int4*, int, bool, int32_t*, int32_t*, int32_t*,      \
-                                      const T*, const T*, T*, T*, cudaStream_t, T*, int32_t*);                     \
+                                      const T*, const T*, T*, T*, cudaStream_t, const int32_t*, T*, int32_t*);     \
   template void launch_permute_in<T>(const double*, int64_t, const int32_t*, T*, int64_t, int64_t, int,            \
                                      cudaStream_t);                                                                \
   template void launch_permute_out<T>(const T*, int64_t, const int32_t*, double*, int64_t, int64_t, int,           \

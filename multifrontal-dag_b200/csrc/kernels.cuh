@@ -214,6 +214,8 @@ void launch_bwd_large(const DevFronts& F, const int32_t* list, int count, int ma
 // front, code, flag base, 0; forward code >= 0: diagonal block, < 0: rest rows chunk -1 - code;
 // backward code: column block).  ticket: zero before the launch; flags: zero before the sweep
 // (one per front and panel step); expired: raised when a bounded wait gives up.
+// test_req (read once per CTA): nonzero makes every wait run out after ~1 ms (a test of the
+// expiry path).
 // Backward: tasks with code < 0 are partial sums of update-row chunk j (kBwdRestRows rows)
 // against column block s (code = -1 - (s << 16 | j)), written to part (front base in the
 // task's fourth int) and counted in counters (one per front and step); code >= 0 is the
@@ -222,7 +224,7 @@ constexpr int kBwdRestRows = 256;
 template <typename T>
 void launch_large_fused(const DevFronts& F, const int4* tasks, int ntask, bool backward, int32_t* ticket,
                         int32_t* flags, int32_t* expired, const T* panel, const T* dinv, T* X, T* V, cudaStream_t st,
-                        T* part = nullptr, int32_t* counters = nullptr);
+                        const int32_t* test_req, T* part = nullptr, int32_t* counters = nullptr);
 // pdl: the single-RHS step kernels go out with programmatic dependent launch
 // (each waits for its predecessor before reading the sweep's vectors)
 

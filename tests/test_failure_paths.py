@@ -5,6 +5,9 @@
   arrives at (a ~1 ms limit) before it issues any MMA.  The factorization must
   return MFD_E_TIMEOUT (-4), refuse a solve, and factor normally once the
   request is withdrawn, on the same handle.
+* The same request makes the single-RHS large-front solve sweeps' flag waits
+  run out: the solve returns MFD_E_TIMEOUT and the handle solves normally
+  once the request is withdrawn.
 * A non-positive pivot in the blocked large-front path and in the fused
   small-front path: the returned info is the pivot's 1-based column, the same
   column the oracle's LAPACK-convention check reports.
@@ -42,13 +45,36 @@ def test_expired_wait_reports_timeout_and_handle_recovers():
     assert P.backward_error(p.n, p.col, p.row, p.val, x, p.rhs) <= 1e-12
 
 
-def test_expire_request_leaves_fp64_alone():
-    """The request only concerns the FP32 tensor-core update: an FP64 handle
-    factors normally with it set."""
+def test_expire_request_leaves_fp64_factor_alone():
+    """In the factorization the request only concerns the FP32 tensor-core
+    update: an FP64 handle factors normally with it set."""
     p = P.laplace3d(12)
     s = H.Solver.analyze(p.n, p.col, p.row, p.order, max_zero=10, small_front_max=48)
     s.test_expire_waits(True)
     assert s.factorize(p.val) == 0
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_expired_solve_wait_reports_timeout_and_handle_recovers(precision):
+    """The single-RHS large-front solve sweeps (one launch per level, tasks
+    waiting on other tasks' flags) under the request: their waits look for a
+    value nothing writes and give up after ~1 ms; the solve returns
+    MFD_E_TIMEOUT (-4) within seconds, and once the request is withdrawn the
+    same handle, without refactoring, solves to backward error <= 1e-12."""
+    p = P.laplace3d(16)
+    s = H.Solver.analyze(p.n, p.col, p.row, p.order, max_zero=1000, small_front_max=48, precision=precision)
+    assert s.factorize(p.val) == 0
+    s.test_expire_waits(True)
+    t0 = time.perf_counter()
+    with pytest.raises(H.MfdError) as e:
+        s.solve(p.rhs.copy())
+    assert e.value.code == -4
+    assert time.perf_counter() - t0 < 30.0              # every wait is bounded
+    s.test_expire_waits(False)
+    x = p.rhs.copy()
+    rep, rc = s.solve(x)
+    assert rc == 0
+    assert P.backward_error(p.n, p.col, p.row, p.val, x, p.rhs) <= 1e-12
 
 
 @pytest.mark.parametrize("small_max", [0, 48])

@@ -249,6 +249,39 @@ def test_deferred_updates_bitwise_equal(precision):
     assert np.abs(x1 - xo).max() <= (FP64_X_TOL if precision == 0 else 1e-8) * np.abs(xo).max()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("mk", [lambda: P.laplace3d(24), lambda: P.diffusion3d(16)], ids=["lap3d24", "diff3d16"])
+def test_fused_solve_sweeps_match_per_step(mk, precision):
+    """The single-RHS large-front sweeps run as one launch per level (tasks in
+    dependency order, device flags; the update rows of the backward sweep in
+    256-row chunk tasks) and, with reserved[6] = 1, one launch per panel step.
+    Both give the oracle's solution (FP64: within the FP64 tolerance; FP32 +
+    refinement: backward error <= 1e-12), agree with each other, and the fused
+    form is deterministic (a second solve is bit-identical)."""
+    p = mk()
+    o = oracle_for(p, max_zero=1000)
+    xs = {}
+    for per_step in (0, 1):
+        s = gpu_for(p, max_zero=1000, small_front_max=48, precision=precision,
+                    reserved=(0, 0, 0, 0, 0, 0, per_step))
+        x = p.rhs.copy()
+        rep, rc = s.solve(x)
+        assert rc == 0 and rep.backward_error <= FP64_BWD_TOL
+        assert P.backward_error(p.n, p.col, p.row, p.val, x, p.rhs) <= FP64_BWD_TOL
+        if per_step == 0:
+            x2 = p.rhs.copy()
+            s.solve(x2)
+            assert np.array_equal(x, x2)
+        xs[per_step] = x
+        s.close()
+    xo = o.solve(p.rhs)
+    scale = np.abs(xo).max()
+    for x in xs.values():
+        # FP32 + refinement stops at backward error 1e-12: its forward error scales with the conditioning
+        assert np.abs(x - xo).max() / scale <= (FP64_X_TOL if precision == 0 else 1e-6)
+    assert np.abs(xs[0] - xs[1]).max() / scale <= (FP64_X_TOL if precision == 0 else 1e-6)
+
+
 def test_programmatic_launch_matches():
     """Programmatic dependent launch along the panel chain (opt-in) gives the
     same factor as the default schedule."""

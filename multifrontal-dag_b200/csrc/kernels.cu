@@ -595,7 +595,7 @@ __global__ void __launch_bounds__(256) k_extend_add_ilp(DevFronts F, const int32
 //      (DMMA).
 // Then the full inverse X = L^{-1}: X_bb = D_b and, per block row r,
 // X_rc = -D_r (sum_{k=c}^{r-1} L_rk X_kc), two warps per block column c; the
-// off-diagonal X blocks are kept transposed in the strict upper part of S.
+// off-diagonal X blocks are kept in the strict upper part of S (block (c, r) holds X_rc).
 // L goes to the panel, X (column-major, ld 128, zero outside the lower w x w;
 // persistent blocks are zeroed at allocation and written on that part only)
 // to linv.  A non-positive pivot records its 1-based column in info (atomic
@@ -909,7 +909,8 @@ __global__ void __launch_bounds__(potrf_threads<NSB>(), 1) k_potrf(DevFronts F, 
     }
     __syncthreads();
   }
-  // ---- inverse: X_rc = -D_r sum_{k=c}^{r-1} L_rk X_kc, X_rc stored transposed at S(32c + j, 32r + i);
+  // ---- inverse: X_rc = -D_r sum_{k=c}^{r-1} L_rk X_kc, X_rc(i, j) stored at S(32c + i, 32r + j) (the
+  //      free block above the diagonal, not transposed, so the write-out below reads it conflict-free);
   //      two warps per block column c, 16 rows each ----
   for (int r = 1; r < nsb; ++r) {
     const int c = warp >> 1, h = warp & 1;
@@ -920,9 +921,9 @@ __global__ void __launch_bounds__(potrf_threads<NSB>(), 1) k_potrf(DevFronts F, 
       // k = c: X_cc = D_c, B(k', j) = D_c(k', j)
       warp_mm32(acc, S + r * kPSub + 16 * h + c * kPSub * kPLd, 1, kPLd, Dv + (size_t)c * kPSub * kDLd, 1, kDLd,
                 kPSub, lane);
-      for (int k = c + 1; k < r; ++k)   // B(k', j) = X_kc(k', j) = S(32c + j, 32k + k')
-        warp_mm32(acc, S + r * kPSub + 16 * h + k * kPSub * kPLd, 1, kPLd, S + c * kPSub + k * kPSub * kPLd, kPLd,
-                  1, kPSub, lane);
+      for (int k = c + 1; k < r; ++k)   // B(k', j) = X_kc(k', j) = S(32c + k', 32k + j)
+        warp_mm32(acc, S + r * kPSub + 16 * h + k * kPSub * kPLd, 1, kPLd, S + c * kPSub + k * kPSub * kPLd, 1,
+                  kPLd, kPSub, lane);
       acc_store(acc, Y + 16 * h, 1, kDLd, 1.0, lane);
     }
     __syncthreads();
@@ -930,7 +931,7 @@ __global__ void __launch_bounds__(potrf_threads<NSB>(), 1) k_potrf(DevFronts F, 
       double acc[2][4][2];
       acc_zero(acc);
       warp_mm32(acc, Dv + (size_t)r * kPSub * kDLd + 16 * h, 1, kDLd, Y, 1, kDLd, kPSub, lane);
-      acc_store(acc, S + c * kPSub + (r * kPSub + 16 * h) * kPLd, kPLd, 1, -1.0, lane);   // transposed
+      acc_store(acc, S + c * kPSub + 16 * h + r * kPSub * kPLd, 1, kPLd, -1.0, lane);
     }
     __syncthreads();
   }
@@ -950,7 +951,8 @@ __global__ void __launch_bounds__(potrf_threads<NSB>(), 1) k_potrf(DevFronts F, 
     double v = 0.0;
     if (in) {
       const int bi = i / kPSub, bj = j / kPSub;
-      v = bi == bj ? Dv[(size_t)bi * kPSub * kDLd + (i - bi * kPSub) + (j - bj * kPSub) * kDLd] : S[j + i * kPLd];
+      v = bi == bj ? Dv[(size_t)bi * kPSub * kDLd + (i - bi * kPSub) + (j - bj * kPSub) * kDLd]
+                   : S[(bj * kPSub + i - bi * kPSub) + (bi * kPSub + j - bj * kPSub) * kPLd];
     }
     Li[i + (size_t)j * kFactB] = (T)v;
   }

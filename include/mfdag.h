@@ -299,7 +299,9 @@ int mfd_destroy(mfd_handle *h);
  * (1 MiB) plus small tables, held by every GPU that loads the library until the
  * process exits; count > MFD_NOALLOC_MAX_FRONTS is rejected with MFD_E_ARG.
  * The first call on a device looks up the array's device address and sets
- * kernel attributes; make that first call before any stream capture.  All
+ * kernel attributes.  No call can be captured into a CUDA graph: each copies
+ * its tables from host memory and waits for the info read-back, so a call on
+ * a stream that is being captured returns MFD_E_ARG and issues nothing.  All
  * calls share the one array, so calls that overlap on the GPU (other streams,
  * other host threads) race.  Host-synchronous on `stream` (NULL = default). */
 #define MFD_NOALLOC_MAX_FRONTS 8

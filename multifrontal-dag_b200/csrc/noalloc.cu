@@ -85,12 +85,24 @@ extern "C" __attribute__((visibility("default"))) int mfd_factor_fronts_noalloc(
     }
     maxnc = nc[i] > maxnc ? nc[i] : maxnc;
   }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // A capture cannot record the host table copy or the info read-back below,
+  // so a capturing stream is refused before anything is issued on it.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    g_msg = "cannot query the stream's capture status";
+    return MFD_E_ARG;
+  }
+  if (cap != cudaStreamCaptureStatusNone) {
+    g_msg = "the stream is being captured into a CUDA graph; this entry point cannot be captured";
+    return MFD_E_ARG;
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { g_msg = "no current device"; return MFD_E_CUDA; }
   double* scratch = nullptr;
   int rc = scratch_on_device(dev, &scratch);
   if (rc) return rc;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
 
   // front tables in the scratch tail: nc, nr, first, list | panel_off, u_off | info per front
   struct Tables {

@@ -113,3 +113,32 @@ def test_noalloc_reports_the_failing_front():
     # the next call starts from cleared info slots
     t2 = torch.from_numpy(np.tril(good).ravel(order="F").copy()).cuda()
     assert H.factor_fronts_noalloc(t2, [0], [0], [nf], [nf], per_front=True) == [0]
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    """A call on a stream that is being captured into a CUDA graph returns
+    MFD_E_ARG and issues nothing: its host table copy and info read-back cannot
+    be recorded.  The capture around it still completes (the graph replays the
+    one op captured beside the call), the front is untouched, and the next call
+    outside the capture factors it."""
+    import torch
+    n = 64
+    a = dense_spd(n, 5)
+    host = np.tril(a).ravel(order="F").copy()
+    t = torch.from_numpy(host.copy()).cuda()
+    z = torch.zeros(4, dtype=torch.float64, device="cuda")
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        z.add_(1.0)
+        with pytest.raises(H.MfdError) as e:
+            H.factor_fronts_noalloc(t, [0], [0], [n], [n], stream=s.cuda_stream)
+    assert e.value.code == -1                            # MFD_E_ARG
+    g.replay()
+    torch.cuda.synchronize()
+    assert z.cpu().tolist() == [1.0] * 4
+    assert np.array_equal(t.cpu().numpy(), host)
+    assert H.factor_fronts_noalloc(t, [0], [0], [n], [n]) == 0
+    got = np.tril(t.cpu().numpy().reshape(n, n, order="F"))
+    ref = np.linalg.cholesky(a)
+    assert np.abs(got - ref).max() <= FACTOR_TOL * np.abs(ref).max()

@@ -583,8 +583,12 @@ int upload_plan(mfd_handle* h) {
   CK(h->d_lists.upload(h->h_lists, st));
   // the fused sweeps' task entries hold 32-bit partial-sum bases and flag offsets: beyond that
   // range (far larger problems than one GPU holds) the per-step sweeps are used instead
-  if (h->bw_part_elems > INT32_MAX || 3LL * h->solve_flags + 2LL * (int64_t)h->levels.size() + 1 > INT32_MAX)
+  // (their flag array and partial-sum buffer then shrink to nothing)
+  if (h->bw_part_elems > INT32_MAX || 3LL * h->solve_flags + 2LL * (int64_t)h->levels.size() + 1 > INT32_MAX) {
     h->h_stasks.clear();
+    h->bw_part_elems = 0;
+    h->solve_flags = 0;
+  }
   if (!h->h_stasks.empty()) CK(h->d_stasks.upload(h->h_stasks, st));
   // [0] expiry, 2 tickets per level, forward flags, backward flags, backward update-row counters
   CK(h->d_ssync.alloc(1 + 2 * h->levels.size() + 3 * (size_t)h->solve_flags));
